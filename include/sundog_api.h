@@ -1,0 +1,253 @@
+/* sundog_api.h — C ABI of the B200 path tracer (libsundog.so).
+ *
+ * The first block is the drop-in surface: the 27 entry points and four
+ * structs that sundog's scene library (scenes/scenelib.py) binds with ctypes.
+ * Names, argument meaning, return codes and struct layouts are identical to
+ * sundog's src/sundog_api.h (cited per declaration), so existing scene files
+ * run against this library unchanged.
+ *
+ * Conventions kept from the reference ABI (src/sundog_api.h:1-15):
+ *   - scalars cross as double and are narrowed to float once, at entry;
+ *   - "unset, use the renderer default" is NaN for doubles, NULL for
+ *     vectors and -1 for tri-state ints;
+ *   - set_* / validate / probe / render return 0 on success, 1 on error;
+ *     add_* return an id >= 0, or -1 on error; scene_create returns NULL on
+ *     error; the message of the last error on the calling thread is
+ *     available from sundog_last_error();
+ *   - call order is config/registries -> objects -> flames -> explicit
+ *     lights -> render, which freezes the light list as
+ *     [auto NEE area lights in object order][2 per flame][explicit lights].
+ *
+ * The second block holds additive entry points with no counterpart in the
+ * reference; they extend, and never change, the layouts above.
+ */
+#ifndef SUNDOG_B200_API_H
+#define SUNDOG_B200_API_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+#define SUNDOG_API extern "C" __attribute__((visibility("default")))
+#else
+#define SUNDOG_API __attribute__((visibility("default")))
+#endif
+
+#define SUNDOG_OK 0
+#define SUNDOG_ERROR 1
+
+/* ======================= drop-in surface (27 symbols) ===================== */
+
+/* src/sundog_api.h:30 — thread-local message of the last failed call. */
+SUNDOG_API const char* sundog_last_error(void);
+
+typedef struct sundog_scene sundog_scene;
+/* src/sundog_api.h:34-35 — handle lifetime; base_dir resolves relative asset
+ * paths ("." when NULL or empty). */
+SUNDOG_API sundog_scene* sundog_scene_create(const char* base_dir);
+SUNDOG_API void sundog_scene_destroy(sundog_scene*);
+
+/* src/sundog_api.h:38-52 — geometry kinds and transform-step kinds. */
+enum {
+  SUNDOG_GK_SPHERE = 0,
+  SUNDOG_GK_RECT = 1,
+  SUNDOG_GK_DISK = 2,
+  SUNDOG_GK_CYLINDER = 3,
+  SUNDOG_GK_PARABOLA = 4,
+  SUNDOG_GK_MESH = 5,
+};
+enum {
+  SUNDOG_XF_SCALE = 0,
+  SUNDOG_XF_TRANSLATE = 1,
+  SUNDOG_XF_ROTATE_X = 2,
+  SUNDOG_XF_ROTATE_Y = 3,
+  SUNDOG_XF_ROTATE_Z = 4,
+};
+#define SUNDOG_MAT_NONE (-1)    /* src/sundog_api.h:53 face passes rays through */
+#define SUNDOG_MAT_DEFAULT (-2) /* src/sundog_api.h:54 back face = front face */
+
+/* src/sundog_api.h:57-76 — configuration blocks. */
+SUNDOG_API int sundog_set_render(sundog_scene*, int width, int height, int spp,
+                                 int max_depth, double clamp, int64_t seed,
+                                 double exposure, int transparent_shadows);
+SUNDOG_API int sundog_set_camera(sundog_scene*, const double lookfrom[3],
+                                 const double lookat[3], const double up[3],
+                                 double vfov, double aperture, double focus_dist);
+SUNDOG_API int sundog_set_background_solid(sundog_scene*, const double color[3]);
+SUNDOG_API int sundog_set_background_gradient(sundog_scene*, const double horizon[3],
+                                              const double zenith[3]);
+SUNDOG_API int sundog_set_background_envmap(sundog_scene*, const char* file,
+                                            double rotate_deg, double intensity,
+                                            int importance);
+SUNDOG_API int sundog_set_physics(sundog_scene*, const double gravity[3],
+                                  double timestep, double max_time, double friction,
+                                  double restitution, int pos_iters, int vel_iters,
+                                  double sleep_threshold, double stop_time);
+
+/* src/sundog_api.h:79-111 — texture / material / mesh registries. */
+SUNDOG_API int sundog_add_texture_solid(sundog_scene*, const double color[3]);
+SUNDOG_API int sundog_add_texture_checker(sundog_scene*, const double a[3],
+                                          const double b[3], const double scale[2]);
+SUNDOG_API int sundog_add_texture_grid(sundog_scene*, const double a[3],
+                                       const double b[3], const double scale[2],
+                                       double width);
+SUNDOG_API int sundog_add_texture_image(sundog_scene*, const char* file, int srgb);
+SUNDOG_API int sundog_add_material_lambert(sundog_scene*, const double color[3],
+                                           int tex_id);
+SUNDOG_API int sundog_add_material_metal(sundog_scene*, const double color[3],
+                                         int tex_id, double roughness);
+SUNDOG_API int sundog_add_material_dielectric(sundog_scene*, double ior,
+                                              const double absorb[3],
+                                              const double color[3], int tex_id,
+                                              double roughness);
+SUNDOG_API int sundog_add_material_emissive(sundog_scene*, const double color[3],
+                                            int tex_id, double intensity,
+                                            int two_sided);
+SUNDOG_API int sundog_add_material_water(sundog_scene*, double ior,
+                                         const double absorb[3], double wave_amp,
+                                         double wave_freq, const double color[3]);
+SUNDOG_API int sundog_add_material_plastic(sundog_scene*, const double color[3],
+                                           int tex_id, double roughness);
+SUNDOG_API int sundog_add_mesh(sundog_scene*, const char* obj_file,
+                               int smooth_normals, const char* usemtl);
+
+/* src/sundog_api.h:117-138 — objects. Byte layouts are load-bearing: the
+ * ctypes mirrors in scenes/scenelib.py:724-734 must match. */
+typedef struct {
+  int32_t kind; /* SUNDOG_XF_* */
+  double a, b, c;
+} sundog_xform_step;
+
+typedef struct {
+  int32_t dynamic;
+  double density;
+  int32_t has_velocity, has_angular_velocity;
+  double velocity[3], angular_velocity[3];
+  double friction, restitution;
+  double thickness;
+} sundog_physics_body;
+
+SUNDOG_API int sundog_add_object(sundog_scene*, int geom_kind, int mesh_id,
+                                 int mat_front, int mat_back, int cutout_tex_id,
+                                 const sundog_xform_step* steps, int num_steps,
+                                 int nee, const sundog_physics_body* physics);
+
+/* src/sundog_api.h:141-152 — flames and explicit lights. */
+SUNDOG_API int sundog_add_flame(sundog_scene*, const double base[3], double height,
+                                double radius, double intensity, double sigma,
+                                double noise_scale, int64_t seed,
+                                double light_intensity);
+SUNDOG_API int sundog_add_point_light(sundog_scene*, const double position[3],
+                                      const double intensity[3], double radius);
+SUNDOG_API int sundog_add_distant_light(sundog_scene*, const double direction[3],
+                                        const double radiance[3]);
+
+/* src/sundog_api.h:155 — GPU-free checks (camera present). */
+SUNDOG_API int sundog_scene_validate(sundog_scene*);
+
+/* src/sundog_api.h:157-165 — device probe. This library has no OptiX: both
+ * OptiX fields are reported as 0. */
+typedef struct {
+  char name[256];
+  int32_t cc_major, cc_minor;
+  int32_t driver_version, runtime_version;
+  uint64_t total_mem_mb;
+  uint32_t optix_header_version;
+  uint32_t rtcore_version;
+} sundog_device_info;
+SUNDOG_API int sundog_probe(sundog_device_info* out);
+
+/* src/sundog_api.h:167-179 — synchronous render of the scene. */
+typedef struct {
+  const char* out_path;
+  const char* stats_path;
+  const char* aov_albedo_path, *aov_normal_path;
+  const char* scene_name;
+  int32_t spp, width, height;
+  int64_t seed;
+  int32_t denoise, transparent_shadows;
+  double clamp;
+  double physics_time;
+  int32_t quiet;
+} sundog_render_options;
+SUNDOG_API int sundog_render(sundog_scene*, const sundog_render_options*);
+
+/* ===================== additive entry points (no reference) =============== */
+
+/* Flame ray-march step count. The reference hard-codes 32 steps in both the
+ * radiance and the shadow marcher; this sets a per-flame count (1..1024) that
+ * both marchers use, default 32. Flames phase; returns 0/1. */
+SUNDOG_API int sundog_set_flame_steps(sundog_scene*, int flame_id, int steps);
+
+/* Extended render: same scene, same options, plus host buffers to receive the
+ * film and a result record. Any pointer may be NULL. film_rgba receives
+ * width*height float4 (linear radiance, running mean over all samples);
+ * aov_albedo / aov_normal likewise (AOVs are accumulated only when one of the
+ * two is non-NULL or the options name AOV paths). out_path may be NULL here,
+ * in which case no image file is written. */
+typedef struct {
+  float* film_rgba;
+  float* aov_albedo;
+  float* aov_normal;
+  int32_t chunk_spp;     /* samples per persistent launch; <= 0 = automatic */
+  int32_t repeat;        /* >1: re-render the film this many times and report
+                            the fastest render loop (timing aid); 0/1 = once */
+  int32_t guiding;       /* 1 = learned path guiding (see sundog_guiding_*) */
+  int32_t reserved;
+} sundog_render_ext;
+
+typedef struct {
+  uint64_t rays_traced;      /* radiance + shadow traces (reference definition) */
+  uint64_t paths;            /* camera samples traced */
+  double render_ms;          /* render loop only (device work, synchronised) */
+  double build_ms;           /* acceleration-structure + CDF build */
+  double load_ms;            /* asset load (OBJ / HDR) */
+  double total_ms;
+  double mrays_per_sec;
+  double samples_per_sec;
+  uint64_t kernel_launches;  /* kernels this library launched in the render loop */
+  double kernel_ms;          /* CUDA-event time of the path-tracing kernels only */
+} sundog_render_result;
+
+SUNDOG_API int sundog_render_ex(sundog_scene*, const sundog_render_options*,
+                                const sundog_render_ext*, sundog_render_result*);
+
+/* Resident render session: the load-time work of sundog_render (asset load,
+ * CDFs, BVH build, uploads) done once, then any number of device-resident
+ * renders of the same film. session_render runs on the given CUDA stream
+ * (NULL = the session's own) and returns when the render is complete;
+ * reset != 0 clears the film first. session_read copies film / AOVs
+ * (width*height float4 each) to host memory. */
+typedef struct sundog_session sundog_session;
+typedef struct {
+  int32_t width, height, spp, chunk_spp;
+  int32_t grid, block;           /* persistent launch shape */
+  uint64_t device_bytes;         /* device memory held by the session */
+  uint64_t bvh_nodes, triangles, instances;
+  int32_t tlas_depth, blas_depth;
+  double load_ms, build_ms, setup_ms;
+} sundog_session_stats;
+
+SUNDOG_API sundog_session* sundog_session_create(sundog_scene*, const sundog_render_options*,
+                                                 const sundog_render_ext*);
+SUNDOG_API int sundog_session_render(sundog_session*, void* cuda_stream, int reset,
+                                     sundog_render_result*);
+SUNDOG_API int sundog_session_read(sundog_session*, float* film_rgba, float* aov_albedo,
+                                   float* aov_normal);
+SUNDOG_API int sundog_session_info(sundog_session*, sundog_session_stats*);
+SUNDOG_API void sundog_session_destroy(sundog_session*);
+
+/* Derived scene state as JSON (lights after NEE registration, object
+ * transforms, materials, flames, settings). Writes at most cap bytes including
+ * the terminating NUL; *needed receives the full length + 1. Returns 0/1. */
+SUNDOG_API int sundog_scene_debug_json(sundog_scene*, char* buf, size_t cap,
+                                       size_t* needed);
+
+/* Device self-test of one hot-path function over a batch of inputs, for
+ * parity tests against the CPU oracle. `which` selects the function (see
+ * sundog_b200/csrc/selftest.cu); in/out are host arrays of documented
+ * per-item layout; n is the item count. Returns 0/1. */
+SUNDOG_API int sundog_selftest(int which, const void* in, int n, void* out,
+                               size_t out_bytes);
+
+#endif /* SUNDOG_B200_API_H */

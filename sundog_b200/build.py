@@ -1,0 +1,97 @@
+"""Build recipe for libsundog.so (sm_100a) — compiled in-tree so the shared
+library travels with the repository.
+
+CUDA translation units go through nvcc with -gencode arch=compute_100a,
+code=sm_100a; host C++ through g++ with FP contraction off, so host-side scene
+derivation and CDF builds round exactly like a plain IEEE build. Everything
+links into sundog_b200/lib/libsundog.so against the static CUDA runtime.
+"""
+
+import os
+import subprocess
+import sys
+import hashlib
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "lib")
+LIB = os.path.join(OUT_DIR, "libsundog.so")
+OBJ_DIR = os.path.join(HERE, "_build")
+
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+
+CU_SOURCES = ["pt_kernel.cu", "selftest.cu", "guide.cu", "serve.cu"]
+CPP_SOURCES = ["scene_api.cpp", "scene_derive.cpp", "assets.cpp", "bvh_build.cpp",
+               "render.cpp", "render_api.cpp"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+                     "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
+                     "-Xptxas", "-warn-spills"]
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off",
+             "-Wall", "-Wno-unused-function", "-I" + os.path.join(CUDA_HOME, "include")]
+
+
+def _sources():
+    return [s for s in CU_SOURCES + CPP_SOURCES if os.path.exists(os.path.join(CSRC, s))]
+
+
+def _digest(path, extra):
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        h.update(f.read())
+    for e in extra:
+        h.update(e.encode())
+    return h.hexdigest()[:16]
+
+
+def _headers_digest():
+    h = hashlib.sha256()
+    for d in (CSRC, os.path.join(HERE, "..", "include")):
+        for name in sorted(os.listdir(d)):
+            if name.endswith((".h", ".cuh")):
+                with open(os.path.join(d, name), "rb") as f:
+                    h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout)
+        raise RuntimeError("build failed: " + " ".join(cmd[:3]) + " ...")
+    return r.stdout
+
+
+def build(verbose=False, force=False):
+    """Compile every translation unit (cached by content hash) and link."""
+    os.makedirs(OUT_DIR, exist_ok=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    hdr = _headers_digest()
+    objs = []
+    for src in _sources():
+        path = os.path.join(CSRC, src)
+        is_cu = src.endswith(".cu")
+        flags = NVCC_FLAGS if is_cu else CXX_FLAGS
+        tag = _digest(path, flags + [hdr])
+        obj = os.path.join(OBJ_DIR, "%s.%s.o" % (src, tag))
+        if force or not os.path.exists(obj):
+            if is_cu:
+                cmd = [NVCC] + flags + ["-c", path, "-o", obj]
+            else:
+                cmd = ["g++"] + flags + ["-c", path, "-o", obj]
+            out = _run(cmd, verbose)
+            if verbose and out.strip():
+                print(out)
+        objs.append(obj)
+    link = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static",
+                                                               "-Xlinker", "-soname=libsundog.so"]
+    _run(link, verbose)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

@@ -1,0 +1,597 @@
+// Render orchestration: sundog_probe, sundog_render (drop-in) and the
+// additive session API that keeps a scene resident on the device.
+//
+// A session does the reference's load-time steps once (src/capi_render.cpp:
+// 74-221): render overrides, OBJ / HDR / image loading, mesh-light CDFs in
+// FP64 (126-172), environment CDFs in FP64 (src/env_light.cpp:27-56), BVH
+// build (host SAH, replacing the OptiX GAS/IAS builds at 175-185) and the
+// uploads. Each session_render then runs the sample loop on the device:
+// per chunk one persistent path-tracing launch plus one film fold.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sundog_api.h"
+#include "abi_util.h"
+#include "assets.h"
+#include "bvh_build.h"
+#include "kernels.h"
+#include "render_session.h"
+#include "scene_model.h"
+
+using namespace sdb;
+using Clock = std::chrono::steady_clock;
+
+namespace sdb {
+
+static double msSince(Clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+
+void cudaCheck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+void DevBuf::alloc(size_t n) {
+  release();
+  if (n == 0) return;
+  cudaCheck(cudaMalloc(&ptr, n), "cudaMalloc");
+  bytes = n;
+}
+void DevBuf::upload(const void* src, size_t n) {
+  alloc(n);
+  if (n) cudaCheck(cudaMemcpy(ptr, src, n, cudaMemcpyHostToDevice), "upload");
+}
+void DevBuf::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+static std::string resolvePath(const SceneDesc& s, const std::string& p) {
+  if (!p.empty() && p[0] != '/') return s.baseDir + "/" + p;
+  return p;
+}
+
+// Inverse of a 3x4 affine map, computed in double and rounded once.
+static void invertAffine(const Xform& x, float4 out[3]) {
+  const float* m = x.m;
+  double a = m[0], b = m[1], c = m[2], d = m[4], e = m[5], f = m[6], g = m[8], h = m[9], i = m[10];
+  double A = e * i - f * h, B = -(d * i - f * g), C = d * h - e * g;
+  double det = a * A + b * B + c * C;
+  if (det == 0.0) throw std::runtime_error("scene: object transform is singular");
+  double inv[9] = {A / det,
+                   -(b * i - c * h) / det,
+                   (b * f - c * e) / det,
+                   B / det,
+                   (a * i - c * g) / det,
+                   -(a * f - c * d) / det,
+                   C / det,
+                   -(a * h - b * g) / det,
+                   (a * e - b * d) / det};
+  double t[3] = {m[3], m[7], m[11]};
+  for (int r = 0; r < 3; r++) {
+    double tr = -(inv[r * 3] * t[0] + inv[r * 3 + 1] * t[1] + inv[r * 3 + 2] * t[2]);
+    out[r] = make_float4((float)inv[r * 3], (float)inv[r * 3 + 1], (float)inv[r * 3 + 2], (float)tr);
+  }
+}
+
+// Equirect CDFs over luminance * sin(theta), FP64 prefix sums stored as
+// float with the last entry pinned to 1; all-black rows get a uniform ramp.
+// (src/env_light.cpp:27-56)
+void buildEnvCdf(const float* rgba, int w, int h, std::vector<float>& marg, std::vector<float>& cond,
+                 bool& degenerate) {
+  marg.assign(h + 1, 0.0f);
+  cond.assign((size_t)h * (w + 1), 0.0f);
+  double total = 0.0;
+  for (int row = 0; row < h; row++) {
+    float sinT = sinf(kPi * (row + 0.5f) / h);
+    float* cdf = &cond[(size_t)row * (w + 1)];
+    double sum = 0.0;
+    cdf[0] = 0.0f;
+    for (int col = 0; col < w; col++) {
+      const float* p = rgba + 4 * ((size_t)row * w + col);
+      float lum = 0.2126f * p[0] + 0.7152f * p[1] + 0.0722f * p[2];
+      sum += (double)fmaxf(lum, 0.0f) * sinT;
+      cdf[col + 1] = (float)sum;
+    }
+    if (sum > 0.0) {
+      for (int c = 1; c <= w; c++) cdf[c] = (float)(cdf[c] / sum);
+    } else {
+      for (int c = 0; c <= w; c++) cdf[c] = (float)c / w;
+    }
+    cdf[w] = 1.0f;
+    total += sum;
+    marg[row + 1] = (float)total;
+  }
+  degenerate = total <= 0.0;
+  if (!degenerate) {
+    for (int r = 1; r <= h; r++) marg[r] = (float)(marg[r] / total);
+  } else {
+    for (int r = 0; r <= h; r++) marg[r] = (float)r / h;
+  }
+  marg[h] = 1.0f;
+}
+
+// World-space triangle-area CDF of an emissive mesh instance: FP64 running
+// total, entries normalised once, last entry 1. (src/capi_render.cpp:143-155)
+void buildMeshLightCdf(const std::vector<float3>& wp, const std::vector<uint3>& idx,
+                       std::vector<float>& cdf, double& total) {
+  size_t n = idx.size();
+  cdf.assign(n + 1, 0.0f);
+  total = 0.0;
+  for (size_t t = 0; t < n; t++) {
+    const uint3& tr = idx[t];
+    total += 0.5 * (double)len(cross(wp[tr.y] - wp[tr.x], wp[tr.z] - wp[tr.x]));
+    cdf[t + 1] = (float)total;
+  }
+  if (!(total > 0.0)) return;
+  for (size_t t = 1; t < n; t++) cdf[t] = (float)(cdf[t] / total);
+  cdf[n] = 1.0f;
+}
+
+static int strataFor(int spp) {  // device/programs.cu:317-319
+  int n = (int)floorf(sqrtf((float)spp) + 0.5f);
+  if (n * n > spp) n--;
+  if (n < 1) n = 1;
+  return n;
+}
+
+RenderSession::~RenderSession() {
+  if (stream) cudaStreamDestroy(stream);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+}
+
+void RenderSession::build(const sundog_scene* h, const sundog_render_options* opt,
+                          const sundog_render_ext* ext) {
+  auto tTotal = Clock::now();
+  scene = h->scene;
+  quiet = opt && opt->quiet != 0;
+  // ---- overrides (src/capi_render.cpp:74-83) ----
+  RenderCfg& rs = scene.render;
+  if (opt) {
+    if (opt->spp > 0) rs.spp = opt->spp;
+    if (opt->width > 0) rs.width = opt->width;
+    if (opt->height > 0) rs.height = opt->height;
+    if (opt->seed >= 0) rs.seed = (unsigned)opt->seed;
+    if (opt->denoise >= 0) rs.denoise = opt->denoise == 1;
+    if (opt->transparent_shadows >= 0) rs.transparentShadows = opt->transparent_shadows == 1;
+    if (!std::isnan(opt->clamp) && opt->clamp >= 0.0) rs.clampVal = (float)opt->clamp;
+    float pt = std::isnan(opt->physics_time) ? -1.0f : (float)opt->physics_time;
+    if (pt >= 0.0f && !scene.physics.enabled)
+      throw std::runtime_error("--physics-time: scene has no physics block");
+  }
+  if (rs.width <= 0 || rs.height <= 0 || rs.spp <= 0) throw std::runtime_error("render: bad size");
+  if (scene.physics.enabled && !quiet)
+    std::fprintf(stderr,
+                 "sundog: physics settling is not part of this renderer; rendering authored "
+                 "poses\n");
+  aov = (opt && (opt->aov_albedo_path || opt->aov_normal_path)) ||
+        (ext && (ext->aov_albedo || ext->aov_normal));
+  int devId = 0;
+  cudaCheck(cudaGetDevice(&devId), "cudaGetDevice");
+  cudaCheck(cudaFree(nullptr), "CUDA context");
+  size_t freeB = 0, totB = 0;
+  cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
+  freeBefore = freeB;
+  cudaCheck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+  cudaCheck(cudaEventCreate(&ev0), "event");
+  cudaCheck(cudaEventCreate(&ev1), "event");
+
+  // ---- assets ----
+  auto tLoad = Clock::now();
+  std::vector<HostMesh> meshes;
+  meshTriangles = 0;
+  for (const MeshCfg& mc : scene.meshes) {
+    meshes.push_back(loadObj(resolvePath(scene, mc.file), mc.smooth, mc.usemtl));
+    meshTriangles += meshes.back().idx.size();
+  }
+  std::vector<SdTexture> texDescs;
+  for (const TextureCfg& tc : scene.textures) {
+    SdTexture d = tc.desc;
+    if (d.kind == TX_IMAGE) {
+      int w = 0, hh = 0;
+      std::vector<unsigned char> px;
+      std::string err;
+      std::string p = resolvePath(scene, tc.file);
+      if (!loadImageRgba8(p, w, hh, px, err))
+        throw std::runtime_error("cannot load texture " + p + ": " + err);
+      texImages.emplace_back();
+      texImages.back().upload(px.data(), px.size());
+      d.img = (const uchar4*)texImages.back().ptr;
+      d.imgW = w;
+      d.imgH = hh;
+      d.srgb = tc.srgb ? 1 : 0;
+    }
+    texDescs.push_back(d);
+  }
+  SdEnv env{};
+  std::vector<float> envRgba;
+  int envW = 0, envH = 0;
+  if (scene.bgKind == BG_ENVMAP) {
+    std::string p = resolvePath(scene, scene.env.file);
+    std::string err;
+    if (!loadHdr(p, envW, envH, envRgba, err))
+      throw std::runtime_error("cannot load envmap '" + p + "' (" + err + ")");
+  }
+  loadMs = msSince(tLoad);
+
+  // ---- CDFs + BVH (the reference's "gas_build" segment) ----
+  auto tBuild = Clock::now();
+  if (scene.bgKind == BG_ENVMAP) {
+    std::vector<float> marg, cond;
+    bool degenerate = false;
+    buildEnvCdf(envRgba.data(), envW, envH, marg, cond, degenerate);
+    if (degenerate && scene.env.importance)
+      std::fprintf(stderr, "envmap: %s has zero luminance, falling back to uniform sampling\n",
+                   scene.env.file.c_str());
+    envTex.upload(envRgba.data(), envRgba.size() * sizeof(float));
+    envMarg.upload(marg.data(), marg.size() * sizeof(float));
+    envCond.upload(cond.data(), cond.size() * sizeof(float));
+    env.texels = (const float4*)envTex.ptr;
+    env.margCdf = (const float*)envMarg.ptr;
+    env.condCdf = (const float*)envCond.ptr;
+    env.width = envW;
+    env.height = envH;
+    env.rotate = scene.env.rotateDeg * kPi / 180.0f;
+    env.intensity = scene.env.intensity;
+    env.importance = (scene.env.importance && !degenerate) ? 1 : 0;
+  }
+
+  // Mesh data on the device.
+  std::vector<SdMesh> meshDescs(meshes.size());
+  meshBufs.resize(meshes.size());
+  for (size_t i = 0; i < meshes.size(); i++) {
+    const HostMesh& m = meshes[i];
+    MeshBufs& mb = meshBufs[i];
+    mb.pos.upload(m.pos.data(), m.pos.size() * sizeof(float3));
+    mb.idx.upload(m.idx.data(), m.idx.size() * sizeof(uint3));
+    if (!m.nrm.empty()) mb.nrm.upload(m.nrm.data(), m.nrm.size() * sizeof(float3));
+    if (!m.uv.empty()) mb.uv.upload(m.uv.data(), m.uv.size() * sizeof(float2));
+    meshDescs[i].pos = (const float3*)mb.pos.ptr;
+    meshDescs[i].idx = (const uint3*)mb.idx.ptr;
+    meshDescs[i].nrm = (const float3*)mb.nrm.ptr;
+    meshDescs[i].uv = (const float2*)mb.uv.ptr;
+    meshDescs[i].numTris = (int)m.idx.size();
+  }
+
+  // Mesh lights: render-local copy of the light list with world geometry.
+  std::vector<SdLight> lights = scene.lights;
+  for (const ObjectCfg& o : scene.objects) {
+    if (o.kind != GK_MESH || o.lightId < 0) continue;
+    const HostMesh& m = meshes[o.mesh];
+    std::vector<float3> wp(m.pos.size());
+    for (size_t i = 0; i < wp.size(); i++) wp[i] = o.xform.point(m.pos[i]);
+    std::vector<float> cdf;
+    double total = 0.0;
+    buildMeshLightCdf(wp, m.idx, cdf, total);
+    if (!(total > 0.0))
+      throw std::runtime_error("mesh NEE light has zero surface area: " + scene.meshes[o.mesh].file);
+    lightBufs.emplace_back();
+    lightBufs.back().upload(wp.data(), wp.size() * sizeof(float3));
+    const float3* dpos = (const float3*)lightBufs.back().ptr;
+    lightBufs.emplace_back();
+    lightBufs.back().upload(cdf.data(), cdf.size() * sizeof(float));
+    SdLight& ld = lights[o.lightId];
+    ld.mPos = dpos;
+    ld.mCdf = (const float*)lightBufs.back().ptr;
+    ld.mIdx = meshDescs[o.mesh].idx;
+    ld.mUv = meshDescs[o.mesh].uv;
+    ld.mNumTris = (int)m.idx.size();
+    ld.area = (float)total;
+    ld.mNgSign = orientSign(o.xform.vec(v3(1, 0, 0)), o.xform.vec(v3(0, 1, 0)),
+                            o.xform.vec(v3(0, 0, 1)));
+  }
+
+  // BLAS per mesh, TLAS over objects.
+  std::vector<BvhNode> allNodes;
+  std::vector<float4> allTris;
+  int nObj = (int)scene.objects.size();
+  std::vector<Box3> instBoxes(nObj);
+  for (int i = 0; i < nObj; i++) {
+    const ObjectCfg& o = scene.objects[i];
+    Box3 b = boxEmpty();
+    if (o.kind == GK_MESH) {
+      for (const float3& p : meshes[o.mesh].pos) boxGrow(b, o.xform.point(p));
+    } else {
+      float3 lo, hi;
+      quadricBoundsHost(o.kind, lo, hi);
+      for (int c = 0; c < 8; c++)
+        boxGrow(b, o.xform.point(v3(c & 1 ? hi.x : lo.x, c & 2 ? hi.y : lo.y, c & 4 ? hi.z : lo.z)));
+    }
+    instBoxes[i] = b;
+  }
+  BvhBuild tlas = buildBvh(instBoxes, 1, 0, 0);
+  allNodes = tlas.nodes;
+  tlasDepth = tlas.maxDepth;
+  blasDepth = 0;
+  for (size_t i = 0; i < meshes.size(); i++) {
+    const HostMesh& m = meshes[i];
+    std::vector<Box3> tb(m.idx.size());
+    for (size_t t = 0; t < m.idx.size(); t++) {
+      Box3 b = boxEmpty();
+      boxGrow(b, m.pos[m.idx[t].x]);
+      boxGrow(b, m.pos[m.idx[t].y]);
+      boxGrow(b, m.pos[m.idx[t].z]);
+      tb[t] = b;
+    }
+    int nodeBase = (int)allNodes.size();
+    int primBase = (int)(allTris.size() / 3);
+    BvhBuild bl = buildBvh(tb, 4, nodeBase, primBase);
+    blasDepth = std::max(blasDepth, bl.maxDepth);
+    meshDescs[i].root = nodeBase;
+    allNodes.insert(allNodes.end(), bl.nodes.begin(), bl.nodes.end());
+    for (int k : bl.order) {
+      const uint3& t = m.idx[k];
+      float3 a = m.pos[t.x], b = m.pos[t.y], c = m.pos[t.z];
+      int ki = k;
+      float kf;
+      std::memcpy(&kf, &ki, sizeof kf);
+      allTris.push_back(make_float4(a.x, a.y, a.z, kf));
+      allTris.push_back(make_float4(b.x, b.y, b.z, 0.0f));
+      allTris.push_back(make_float4(c.x, c.y, c.z, 0.0f));
+    }
+  }
+  // Instances in TLAS leaf order (leaf start = position in this array).
+  std::vector<SdInstance> inst(nObj);
+  for (int k = 0; k < nObj; k++) {
+    const ObjectCfg& o = scene.objects[tlas.order[k]];
+    SdInstance& in = inst[k];
+    std::memset(&in, 0, sizeof in);
+    invertAffine(o.xform, in.w2o);
+    in.kind = o.kind;
+    in.mesh = o.mesh;
+    in.mats = (uint32_t)o.matFront | ((uint32_t)o.matBack << 16);
+    in.lightId = o.lightId;
+    in.cutoutTex = o.cutoutTex;
+    bool masked = o.matFront == kMatNone || o.matBack == kMatNone || o.cutoutTex >= 0;
+    bool trans = matTransmissive(scene, o.matFront) || matTransmissive(scene, o.matBack);
+    in.flags = (masked ? kInstMasked : 0) | (trans ? kInstTransmissive : 0);
+  }
+  numNodes = allNodes.size();
+  numTris = allTris.size() / 3;
+  dNodes.upload(allNodes.data(), allNodes.size() * sizeof(BvhNode));
+  dTris.upload(allTris.data(), allTris.size() * sizeof(float4));
+  dInst.upload(inst.data(), inst.size() * sizeof(SdInstance));
+  dMeshes.upload(meshDescs.data(), meshDescs.size() * sizeof(SdMesh));
+  dTex.upload(texDescs.data(), texDescs.size() * sizeof(SdTexture));
+  dMat.upload(scene.materials.data(), scene.materials.size() * sizeof(SdMaterial));
+  dLights.upload(lights.data(), lights.size() * sizeof(SdLight));
+  dFlames.upload(scene.flames.data(), scene.flames.size() * sizeof(SdFlame));
+  buildMs = msSince(tBuild);
+
+  // ---- film and per-sample buffers ----
+  size_t npix = (size_t)rs.width * rs.height;
+  accum.alloc(npix * sizeof(float4));
+  if (aov) {
+    aovAlb.alloc(npix * sizeof(float4));
+    aovNrm.alloc(npix * sizeof(float4));
+  }
+  chunk = ext && ext->chunk_spp > 0 ? ext->chunk_spp : 0;
+  if (chunk <= 0) {
+    // Keep the per-sample buffers near 1 GiB.
+    size_t perSample = npix * sizeof(float4) * (aov ? 3 : 1);
+    size_t cap = (size_t)1 << 30;
+    chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)rs.spp, cap / perSample));
+  }
+  chunk = std::min(chunk, rs.spp);
+  sampleL.alloc(npix * chunk * sizeof(float4));
+  if (aov) {
+    sampleAlb.alloc(npix * chunk * sizeof(float4));
+    sampleNrm.alloc(npix * chunk * sizeof(float4));
+  }
+  counters.alloc(2 * sizeof(unsigned long long));
+
+  SdLaunch& l = lp;
+  std::memset(&l, 0, sizeof l);
+  l.width = rs.width;
+  l.height = rs.height;
+  l.sppTotal = rs.spp;
+  l.maxDepth = rs.maxDepth;
+  l.nStrata = strataFor(rs.spp);
+  l.clampVal = rs.clampVal;
+  l.seed = rs.seed;
+  l.transparentShadows = rs.transparentShadows ? 1 : 0;
+  l.aovOn = aov ? 1 : 0;
+  l.tilesX = (rs.width + 7) / 8;
+  int tilesY = (rs.height + 7) / 8;
+  l.npixPad = l.tilesX * tilesY * 64;
+  l.pathCounter = (unsigned long long*)counters.ptr;
+  l.rayCounter = (unsigned long long*)counters.ptr + 1;
+  l.sampleL = (float4*)sampleL.ptr;
+  l.sampleAlb = (float4*)sampleAlb.ptr;
+  l.sampleNrm = (float4*)sampleNrm.ptr;
+  l.accum = (float4*)accum.ptr;
+  l.aovAlbedo = (float4*)aovAlb.ptr;
+  l.aovNormal = (float4*)aovNrm.ptr;
+  l.cam = buildCamera(scene.camera, rs.width, rs.height);
+  l.bgKind = scene.bgKind;
+  l.bgA = scene.bgA;
+  l.bgB = scene.bgB;
+  l.env = env;
+  l.textures = (const SdTexture*)dTex.ptr;
+  l.materials = (const SdMaterial*)dMat.ptr;
+  l.lights = (const SdLight*)dLights.ptr;
+  l.numLights = (int)lights.size();
+  l.flames = (const SdFlame*)dFlames.ptr;
+  l.numFlames = (int)scene.flames.size();
+  l.nodes = (const BvhNode*)dNodes.ptr;
+  l.tris = (const float4*)dTris.ptr;
+  l.inst = (const SdInstance*)dInst.ptr;
+  l.meshes = (const SdMesh*)dMeshes.ptr;
+  l.tlasRoot = 0;
+  l.numInstances = nObj;
+  grid = renderGridSize();
+  cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
+  deviceBytes = freeBefore > freeB ? freeBefore - freeB : 0;
+  setupMs = msSince(tTotal);
+}
+
+void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* res) {
+  if (!st) st = stream;
+  size_t npix = (size_t)lp.width * lp.height;
+  if (reset) {
+    cudaCheck(cudaMemsetAsync(accum.ptr, 0, accum.bytes, st), "film reset");
+    if (aov) {
+      cudaCheck(cudaMemsetAsync(aovAlb.ptr, 0, aovAlb.bytes, st), "film reset");
+      cudaCheck(cudaMemsetAsync(aovNrm.ptr, 0, aovNrm.bytes, st), "film reset");
+    }
+  }
+  cudaCheck(cudaMemsetAsync(lp.rayCounter, 0, sizeof(unsigned long long), st), "counter reset");
+  cudaCheck(cudaStreamSynchronize(st), "sync");
+  auto t0 = Clock::now();
+  cudaCheck(cudaEventRecord(ev0, st), "event");
+  uint64_t launches = 0;
+  int done = 0;
+  while (done < lp.sppTotal) {
+    int n = std::min(chunk, lp.sppTotal - done);
+    lp.sampleOffset = done;
+    lp.sppThisLaunch = n;
+    lp.numPaths = (unsigned long long)lp.npixPad * n;
+    cudaCheck(cudaMemsetAsync(lp.pathCounter, 0, sizeof(unsigned long long), st), "counter reset");
+    cudaCheck(setLaunch(lp, st), "launch params");
+    cudaCheck(launchRender(st, grid), "path kernel launch");
+    cudaCheck(launchFold((int)npix, st), "fold launch");
+    launches += 2;
+    done += n;
+  }
+  cudaCheck(cudaEventRecord(ev1, st), "event");
+  cudaCheck(cudaStreamSynchronize(st), "path kernels");
+  double wall = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+  float evMs = 0.0f;
+  cudaCheck(cudaEventElapsedTime(&evMs, ev0, ev1), "event time");
+  unsigned long long rays = 0;
+  cudaCheck(cudaMemcpy(&rays, lp.rayCounter, sizeof rays, cudaMemcpyDeviceToHost), "ray count");
+  lastRays = rays;
+  lastRenderMs = wall;
+  lastKernelMs = evMs;
+  if (res) {
+    res->rays_traced = rays;
+    res->paths = (uint64_t)npix * lp.sppTotal;
+    res->render_ms = wall;
+    res->build_ms = buildMs;
+    res->load_ms = loadMs;
+    res->mrays_per_sec = wall > 0 ? rays / wall / 1000.0 : 0.0;
+    res->samples_per_sec = wall > 0 ? (double)npix * lp.sppTotal / (wall / 1000.0) : 0.0;
+    res->kernel_launches = launches;
+    res->kernel_ms = evMs;
+  }
+}
+
+void RenderSession::read(float* film, float* alb, float* nrm) {
+  size_t n = (size_t)lp.width * lp.height * sizeof(float4);
+  if (film) cudaCheck(cudaMemcpy(film, accum.ptr, n, cudaMemcpyDeviceToHost), "film download");
+  if (alb) {
+    if (!aov) throw std::runtime_error("session: AOVs were not requested");
+    cudaCheck(cudaMemcpy(alb, aovAlb.ptr, n, cudaMemcpyDeviceToHost), "aov download");
+  }
+  if (nrm) {
+    if (!aov) throw std::runtime_error("session: AOVs were not requested");
+    cudaCheck(cudaMemcpy(nrm, aovNrm.ptr, n, cudaMemcpyDeviceToHost), "aov download");
+  }
+}
+
+void quadricBoundsHost(int kind, float3& lo, float3& hi) {
+  const float e = 1e-4f;
+  if (kind == GK_RECT || kind == GK_DISK) {
+    lo = v3(-1.0f, -e, -1.0f);
+    hi = v3(1.0f, e, 1.0f);
+  } else if (kind == GK_PARABOLA) {
+    lo = v3(-1.0f, -e, -1.0f);
+    hi = v3(1.0f, 0.5f + e, 1.0f);
+  } else {
+    lo = v3(-1.0f);
+    hi = v3(1.0f);
+  }
+}
+
+}  // namespace sdb
+
+// ---- ABI ---------------------------------------------------------------------
+
+// src/capi_render.cpp:55-77 — device identity; no OptiX in this build.
+extern "C" int sundog_probe(sundog_device_info* out) {
+  SDB_TRY
+  if (!out) throw std::runtime_error("probe: null output");
+  int dev = 0;
+  cudaCheck(cudaGetDevice(&dev), "cudaGetDevice");
+  cudaDeviceProp p;
+  cudaCheck(cudaGetDeviceProperties(&p, dev), "cudaGetDeviceProperties");
+  std::memset(out, 0, sizeof *out);
+  std::snprintf(out->name, sizeof(out->name), "%s", p.name);
+  out->cc_major = p.major;
+  out->cc_minor = p.minor;
+  int dv = 0, rv = 0;
+  cudaDriverGetVersion(&dv);
+  cudaRuntimeGetVersion(&rv);
+  out->driver_version = dv;
+  out->runtime_version = rv;
+  out->total_mem_mb = (uint64_t)(p.totalGlobalMem >> 20);
+  out->optix_header_version = 0;
+  out->rtcore_version = 0;
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" sundog_session* sundog_session_create(sundog_scene* h, const sundog_render_options* opt,
+                                                 const sundog_render_ext* ext) {
+  SDB_TRY
+  if (!h) throw std::runtime_error("render: null scene");
+  if (sundog_scene_validate(h) != SUNDOG_OK) throw std::runtime_error(sundog_last_error());
+  std::unique_ptr<RenderSession> s(new RenderSession());
+  s->build(h, opt, ext);
+  return reinterpret_cast<sundog_session*>(s.release());
+  SDB_CATCH(nullptr)
+}
+
+extern "C" int sundog_session_render(sundog_session* sh, void* stream, int reset,
+                                     sundog_render_result* res) {
+  SDB_TRY
+  if (!sh) throw std::runtime_error("session: null handle");
+  reinterpret_cast<RenderSession*>(sh)->render((cudaStream_t)stream, reset != 0, res);
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_session_read(sundog_session* sh, float* film, float* alb, float* nrm) {
+  SDB_TRY
+  if (!sh) throw std::runtime_error("session: null handle");
+  reinterpret_cast<RenderSession*>(sh)->read(film, alb, nrm);
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_session_info(sundog_session* sh, sundog_session_stats* st) {
+  SDB_TRY
+  if (!sh || !st) throw std::runtime_error("session: null argument");
+  const RenderSession* s = reinterpret_cast<RenderSession*>(sh);
+  st->width = s->lp.width;
+  st->height = s->lp.height;
+  st->spp = s->lp.sppTotal;
+  st->chunk_spp = s->chunk;
+  st->grid = s->grid;
+  st->block = kRenderBlock;
+  st->device_bytes = s->deviceBytes;
+  st->bvh_nodes = s->numNodes;
+  st->triangles = s->numTris;
+  st->instances = (uint64_t)s->lp.numInstances;
+  st->tlas_depth = s->tlasDepth;
+  st->blas_depth = s->blasDepth;
+  st->load_ms = s->loadMs;
+  st->build_ms = s->buildMs;
+  st->setup_ms = s->setupMs;
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" void sundog_session_destroy(sundog_session* sh) {
+  delete reinterpret_cast<RenderSession*>(sh);
+}

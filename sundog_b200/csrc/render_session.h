@@ -1,0 +1,71 @@
+// A scene uploaded to the device and ready to render repeatedly.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/sundog_api.h"
+#include "scene_model.h"
+
+namespace sdb {
+
+void cudaCheck(cudaError_t e, const char* what);
+
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes) {
+    o.ptr = nullptr;
+    o.bytes = 0;
+  }
+  ~DevBuf() { release(); }
+  void alloc(size_t n);
+  void upload(const void* src, size_t n);
+  void release();
+};
+
+struct MeshBufs {
+  DevBuf pos, idx, nrm, uv;
+};
+
+void buildEnvCdf(const float* rgba, int w, int h, std::vector<float>& marg, std::vector<float>& cond,
+                 bool& degenerate);
+void buildMeshLightCdf(const std::vector<float3>& wp, const std::vector<uint3>& idx,
+                       std::vector<float>& cdf, double& total);
+void quadricBoundsHost(int kind, float3& lo, float3& hi);
+
+struct RenderSession {
+  SceneDesc scene;
+  SdLaunch lp{};
+  bool quiet = false;
+  bool aov = false;
+  int chunk = 1;
+  int grid = 0;
+  size_t freeBefore = 0, deviceBytes = 0;
+  size_t meshTriangles = 0, numNodes = 0, numTris = 0;
+  int tlasDepth = 0, blasDepth = 0;
+  double loadMs = 0, buildMs = 0, setupMs = 0;
+  unsigned long long lastRays = 0;
+  double lastRenderMs = 0, lastKernelMs = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  DevBuf envTex, envMarg, envCond;
+  std::vector<DevBuf> texImages;
+  std::vector<MeshBufs> meshBufs;
+  std::vector<DevBuf> lightBufs;
+  DevBuf dNodes, dTris, dInst, dMeshes, dTex, dMat, dLights, dFlames;
+  DevBuf accum, aovAlb, aovNrm, sampleL, sampleAlb, sampleNrm, counters;
+
+  ~RenderSession();
+  void build(const sundog_scene* h, const sundog_render_options* opt, const sundog_render_ext* ext);
+  void render(cudaStream_t st, bool reset, sundog_render_result* res);
+  void read(float* film, float* alb, float* nrm);
+};
+
+}  // namespace sdb

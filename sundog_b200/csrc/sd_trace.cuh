@@ -1,0 +1,386 @@
+// Two-level BVH traversal in software (B200 has no RT cores).
+//
+// One loop walks the instance BVH (TLAS) and, on reaching a mesh instance,
+// the mesh's own BVH (BLAS) with the ray mapped into object space; a marker
+// on the per-thread stack restores the world ray when the BLAS is done.
+// Quadric instances are tested analytically at the TLAS leaf.
+//
+// Hit semantics reproduce what sundog obtains from OptiX
+// (device/programs.cu:49-85, 112-125, 207-302; src/accel.cpp:54-58, 105-107):
+//  * radiance rays: closest accepted hit in (0, tmax); a candidate whose hit
+//    side has no material (MAT_NONE) or whose cutout alpha is < 0.5 is
+//    ignored and traversal continues; every quadric root is a candidate;
+//  * shadow rays: any accepted opaque hit in (0, tmax) occludes; a glass or
+//    water crossing (transparent shadows on) multiplies the Fresnel
+//    transmission 1 - F and adds the signed optical depth +-sigma t, and is
+//    ignored; each crossing is visited exactly once because BVH leaves
+//    partition the primitives.
+// Triangles use the watertight test of Woop, Benthin and Wald (JCGT 2013).
+#pragma once
+
+#include "sd_quadric.cuh"
+#include "sd_texture.cuh"
+#include "sd_types.h"
+
+namespace sdb {
+
+constexpr int kStackSize = 64;
+constexpr int kPop = (int)0x80000000;        // "take the next stack entry"
+constexpr int kToTlas = (int)0x80000001;     // marker: leave the BLAS
+
+struct TraceHit {
+  float t;
+  int inst;
+  int prim;      // mesh-local triangle index (meshes)
+  float u, v;    // triangle barycentrics (weights of p1, p2) or quadric uv
+  float3 nq;     // quadric object-space front normal
+  bool front;
+};
+
+struct ShadePt {
+  float3 nFront;  // world unit normal of the canonical front side
+  float u, v;
+  bool front;
+};
+
+__device__ __forceinline__ float3 ldg3(const float3* p) {
+  const float* f = reinterpret_cast<const float*>(p);
+  return v3(__ldg(f), __ldg(f + 1), __ldg(f + 2));
+}
+
+__device__ __forceinline__ float3 xfPoint(const float4* m, float3 p) {
+  return v3(m[0].x * p.x + m[0].y * p.y + m[0].z * p.z + m[0].w,
+            m[1].x * p.x + m[1].y * p.y + m[1].z * p.z + m[1].w,
+            m[2].x * p.x + m[2].y * p.y + m[2].z * p.z + m[2].w);
+}
+__device__ __forceinline__ float3 xfVec(const float4* m, float3 v) {
+  return v3(m[0].x * v.x + m[0].y * v.y + m[0].z * v.z,
+            m[1].x * v.x + m[1].y * v.y + m[1].z * v.z,
+            m[2].x * v.x + m[2].y * v.y + m[2].z * v.z);
+}
+// Object-space normal to world space: transpose of the world->object map.
+__device__ __forceinline__ float3 xfNormal(const float4* m, float3 n) {
+  return v3(m[0].x * n.x + m[1].x * n.y + m[2].x * n.z,
+            m[0].y * n.x + m[1].y * n.y + m[2].y * n.z,
+            m[0].z * n.x + m[1].z * n.y + m[2].z * n.z);
+}
+
+// Per-ray constants of the watertight triangle test.
+struct WtRay {
+  int kx, ky, kz;
+  float Sx, Sy, Sz;
+};
+__device__ __forceinline__ WtRay wtSetup(float3 d) {
+  WtRay w;
+  float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  w.kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  w.kx = w.kz == 2 ? 0 : w.kz + 1;
+  w.ky = w.kx == 2 ? 0 : w.kx + 1;
+  float dz = comp(d, w.kz);
+  if (dz < 0.0f) {
+    int t = w.kx;
+    w.kx = w.ky;
+    w.ky = t;
+  }
+  w.Sx = comp(d, w.kx) / dz;
+  w.Sy = comp(d, w.ky) / dz;
+  w.Sz = 1.0f / dz;
+  return w;
+}
+
+// Watertight ray/triangle; returns t and the weights (b1, b2) of p1, p2.
+__device__ __forceinline__ bool wtHit(const WtRay& w, float3 o, float3 p0, float3 p1, float3 p2,
+                                      float tmin, float tmax, float& t, float& b1, float& b2) {
+  float3 A = p0 - o, B = p1 - o, C = p2 - o;
+  float Az = comp(A, w.kz), Bz = comp(B, w.kz), Cz = comp(C, w.kz);
+  float Ax = comp(A, w.kx) - w.Sx * Az, Ay = comp(A, w.ky) - w.Sy * Az;
+  float Bx = comp(B, w.kx) - w.Sx * Bz, By = comp(B, w.ky) - w.Sy * Bz;
+  float Cx = comp(C, w.kx) - w.Sx * Cz, Cy = comp(C, w.ky) - w.Sy * Cz;
+  float U = Cx * By - Cy * Bx;
+  float V = Ax * Cy - Ay * Cx;
+  float W = Bx * Ay - By * Ax;
+  if (U == 0.0f || V == 0.0f || W == 0.0f) {
+    // Edge case: redo the 2D edge functions in double (exact for float input).
+    U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+    V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+    W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+  }
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+  float det = U + V + W;
+  if (det == 0.0f) return false;
+  float T = U * (w.Sz * Az) + V * (w.Sz * Bz) + W * (w.Sz * Cz);
+  float inv = 1.0f / det;
+  t = T * inv;
+  if (!(t > tmin && t < tmax)) return false;
+  b1 = V * inv;
+  b2 = W * inv;
+  return true;
+}
+
+// Slab test of both children of a node; robust far-plane scaling after Ize,
+// "Robust BVH Ray Traversal" (JCGT 2013).
+__device__ __forceinline__ void boxPair(const BvhNode& nd, float3 oi, float3 id, float tmin,
+                                        float tmax, float& ta, float& tb, bool& ha, bool& hb) {
+  const float kFar = 1.00000024f;
+  float lx0 = nd.xy0.x * id.x - oi.x, hx0 = nd.xy0.y * id.x - oi.x;
+  float ly0 = nd.xy0.z * id.y - oi.y, hy0 = nd.xy0.w * id.y - oi.y;
+  float lz0 = nd.zz.x * id.z - oi.z, hz0 = nd.zz.y * id.z - oi.z;
+  float lx1 = nd.xy1.x * id.x - oi.x, hx1 = nd.xy1.y * id.x - oi.x;
+  float ly1 = nd.xy1.z * id.y - oi.y, hy1 = nd.xy1.w * id.y - oi.y;
+  float lz1 = nd.zz.z * id.z - oi.z, hz1 = nd.zz.w * id.z - oi.z;
+  float n0 = fmaxf(fmaxf(fminf(lx0, hx0), fminf(ly0, hy0)), fmaxf(fminf(lz0, hz0), tmin));
+  float f0 = fminf(fminf(fmaxf(lx0, hx0), fmaxf(ly0, hy0)), fminf(fmaxf(lz0, hz0), tmax)) * kFar;
+  float n1 = fmaxf(fmaxf(fminf(lx1, hx1), fminf(ly1, hy1)), fmaxf(fminf(lz1, hz1), tmin));
+  float f1 = fminf(fminf(fmaxf(lx1, hx1), fmaxf(ly1, hy1)), fminf(fmaxf(lz1, hz1), tmax)) * kFar;
+  ha = n0 <= f0;
+  hb = n1 <= f1;
+  ta = n0;
+  tb = n1;
+}
+
+__device__ __forceinline__ float safeInv(float x) {
+  const float e = 1e-20f;
+  return 1.0f / (fabsf(x) > e ? x : copysignf(e, x));
+}
+
+__device__ __forceinline__ BvhNode loadNode(const BvhNode* nodes, int i) {
+  const float4* p = reinterpret_cast<const float4*>(nodes + i);
+  BvhNode n;
+  n.xy0 = __ldg(p);
+  n.xy1 = __ldg(p + 1);
+  n.zz = __ldg(p + 2);
+  float4 l = __ldg(p + 3);
+  n.link = make_int4(__float_as_int(l.x), __float_as_int(l.y), __float_as_int(l.z),
+                     __float_as_int(l.w));
+  return n;
+}
+
+// Shade point of a triangle hit (device/programs.cu:147-190): geometric
+// normal through the inverse transpose, interpolated smooth normal kept on
+// the geometric side, uv from the mesh or the barycentrics, and the
+// geometric normal for emissive faces of registered mesh lights.
+__device__ __forceinline__ ShadePt triShade(const SdLaunch& lp, const SdInstance& in, int prim,
+                                            float b1, float b2, float3 D) {
+  const SdMesh& me = lp.meshes[in.mesh];
+  uint3 tri = me.idx[prim];
+  float3 p0 = ldg3(me.pos + tri.x), p1 = ldg3(me.pos + tri.y), p2 = ldg3(me.pos + tri.z);
+  float3 ngObj = cross(p1 - p0, p2 - p0);
+  float3 ng = unit(xfNormal(in.w2o, ngObj));
+  float3 ns = ng;
+  float w0 = 1.0f - b1 - b2;
+  if (me.nrm) {
+    float3 n = ldg3(me.nrm + tri.x) * w0 + ldg3(me.nrm + tri.y) * b1 + ldg3(me.nrm + tri.z) * b2;
+    ns = unit(xfNormal(in.w2o, n));
+    if (dot(ns, ng) < 0.0f) ns = -ns;
+  }
+  ShadePt sp;
+  sp.nFront = ns;
+  if (me.uv) {
+    float2 a = me.uv[tri.x], b = me.uv[tri.y], c = me.uv[tri.z];
+    sp.u = a.x * w0 + b.x * b1 + c.x * b2;
+    sp.v = a.y * w0 + b.y * b1 + c.y * b2;
+  } else {
+    sp.u = b1;
+    sp.v = b2;
+  }
+  sp.front = dot(ng, D) < 0.0f;
+  if (in.lightId >= 0) {
+    uint16_t side = sp.front ? (uint16_t)(in.mats & 0xFFFF) : (uint16_t)(in.mats >> 16);
+    if (side != kMatNone && lp.materials[side].kind == MT_EMISSIVE) sp.nFront = ng;
+  }
+  return sp;
+}
+
+__device__ __forceinline__ ShadePt quadShade(const SdInstance& in, float3 nq, float u, float v,
+                                             float3 D) {
+  ShadePt sp;
+  sp.nFront = unit(xfNormal(in.w2o, nq));
+  sp.u = u;
+  sp.v = v;
+  sp.front = dot(sp.nFront, D) < 0.0f;
+  return sp;
+}
+
+// Any-hit filter shared by both ray types: false = pass through.
+__device__ __forceinline__ bool faceAccepts(const SdLaunch& lp, const SdInstance& in, bool front,
+                                            float u, float v) {
+  uint16_t m = front ? (uint16_t)(in.mats & 0xFFFF) : (uint16_t)(in.mats >> 16);
+  if (m == kMatNone) return false;
+  if (in.cutoutTex >= 0) {
+    float4 c = texLookup(lp.textures[in.cutoutTex], u, v);
+    if (c.w < 0.5f) return false;
+  }
+  return true;
+}
+
+// Transparent-shadow bookkeeping for one crossing; false = the crossing
+// occludes (opaque material, transparent shadows off, or TIR).
+// (device/programs.cu:247-292)
+__device__ __forceinline__ bool shadowCross(const SdLaunch& lp, const ShadePt& sp, uint16_t mid,
+                                            float t, float3 D, float& trProd, float3& tau) {
+  const SdMaterial& m = lp.materials[mid];
+  if (m.kind != MT_DIELECTRIC && m.kind != MT_WATER) return false;
+  if (!lp.transparentShadows) return false;
+  float3 n = sp.front ? sp.nFront : -sp.nFront;
+  float eta = sp.front ? 1.0f / m.ior : m.ior;
+  float3 refr;
+  if (!snell(D, n, eta, refr)) return false;
+  float f0 = (1.0f - eta) / (1.0f + eta);
+  f0 = f0 * f0;
+  float c = sp.front ? -dot(D, n) : -dot(refr, n);
+  float F = fresnelSchlick(c, f0);
+  trProd *= (1.0f - F);
+  float s = sp.front ? -t : t;
+  tau = v3(tau.x + m.absorb.x * s, tau.y + m.absorb.y * s, tau.z + m.absorb.z * s);
+  return true;
+}
+
+// SHADOW = false: closest accepted hit, returns whether one was found.
+// SHADOW = true: returns false when occluded, else accumulates the
+// transparent-crossing terms into trProd / tau.
+template <bool SHADOW>
+__device__ __forceinline__ bool traverse(const SdLaunch& lp, float3 O, float3 D, float tmax,
+                                         TraceHit& hit, float& trProd, float3& tau) {
+  if (lp.numInstances == 0) return SHADOW;
+  int stack[kStackSize];
+  int sp = 0;
+  const BvhNode* nodes = lp.nodes;
+  const float tmin = 0.0f;
+
+  float3 ro = O, rd = D;
+  float3 id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
+  float3 oi = ro * id;
+  WtRay wr;
+  bool inBlas = false;
+  int curInst = -1;
+  bool found = false;
+  int cur = lp.tlasRoot;
+
+  while (true) {
+    if (cur >= 0) {
+      BvhNode nd = loadNode(nodes, cur);
+      float ta, tb;
+      bool ha, hb;
+      boxPair(nd, oi, id, tmin, tmax, ta, tb, ha, hb);
+      if (ha && hb) {
+        int first = nd.link.x, second = nd.link.y;
+        if (tb < ta) {
+          first = nd.link.y;
+          second = nd.link.x;
+        }
+        if (sp < kStackSize) stack[sp++] = second;
+        cur = first;
+      } else if (ha) {
+        cur = nd.link.x;
+      } else if (hb) {
+        cur = nd.link.y;
+      } else {
+        cur = kPop;
+      }
+      continue;
+    }
+    if (cur == kPop) {
+      if (sp == 0) break;
+      cur = stack[--sp];
+      if (cur == kToTlas) {
+        inBlas = false;
+        ro = O;
+        rd = D;
+        id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
+        oi = ro * id;
+        cur = kPop;
+      }
+      continue;
+    }
+    // Leaf: ~cur = start << 3 | (count - 1).
+    int code = ~cur;
+    int start = code >> 3;
+    int count = (code & 7) + 1;
+    cur = kPop;
+    if (!inBlas) {
+      // TLAS leaves hold exactly one instance.
+      const SdInstance& in = lp.inst[start];
+      float3 o2 = xfPoint(in.w2o, O), d2 = xfVec(in.w2o, D);
+      if (in.kind == GK_MESH) {
+        if (sp < kStackSize) {
+          stack[sp++] = kToTlas;
+          inBlas = true;
+          curInst = start;
+          ro = o2;
+          rd = d2;
+          id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
+          oi = ro * id;
+          wr = wtSetup(rd);
+          cur = lp.meshes[in.mesh].root;
+        }
+        continue;
+      }
+      QHits qh = hitQuadric(in.kind, o2, d2, tmin, tmax);
+      for (int k = 0; k < qh.n; k++) {
+        const QHit& q = qh.h[k];
+        if (q.t >= tmax) continue;
+        bool front = dot(q.n, d2) < 0.0f;
+        if ((in.flags & kInstMasked) && !faceAccepts(lp, in, front, q.u, q.v)) continue;
+        if (SHADOW) {
+          if (!(in.flags & kInstTransmissive)) return false;
+          uint16_t mid = front ? (uint16_t)(in.mats & 0xFFFF) : (uint16_t)(in.mats >> 16);
+          ShadePt spt = quadShade(in, q.n, q.u, q.v, D);
+          if (!shadowCross(lp, spt, mid, q.t, D, trProd, tau)) return false;
+        } else {
+          tmax = q.t;
+          found = true;
+          hit.t = q.t;
+          hit.inst = start;
+          hit.prim = 0;
+          hit.u = q.u;
+          hit.v = q.v;
+          hit.nq = q.n;
+          hit.front = front;
+        }
+      }
+      continue;
+    }
+    // BLAS leaf: triangles in object space of curInst.
+    for (int k = 0; k < count; k++) {
+      const float4* tp = lp.tris + 3 * (size_t)(start + k);
+      float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+      float t, b1, b2;
+      float3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
+      if (!wtHit(wr, ro, p0, p1, p2, tmin, tmax, t, b1, b2)) continue;
+      int prim = __float_as_int(a.w);
+      const SdInstance& in = lp.inst[curInst];
+      bool needFace = (in.flags & (kInstMasked | kInstTransmissive)) != 0;
+      if (!needFace) {
+        if (SHADOW) return false;
+        tmax = t;
+        found = true;
+        hit.t = t;
+        hit.inst = curInst;
+        hit.prim = prim;
+        hit.u = b1;
+        hit.v = b2;
+        hit.front = dot(cross(p1 - p0, p2 - p0), rd) < 0.0f;
+        continue;
+      }
+      ShadePt spt = triShade(lp, in, prim, b1, b2, D);
+      if ((in.flags & kInstMasked) && !faceAccepts(lp, in, spt.front, spt.u, spt.v)) continue;
+      if (SHADOW) {
+        if (!(in.flags & kInstTransmissive)) return false;
+        uint16_t mid = spt.front ? (uint16_t)(in.mats & 0xFFFF) : (uint16_t)(in.mats >> 16);
+        if (!shadowCross(lp, spt, mid, t, D, trProd, tau)) return false;
+      } else {
+        tmax = t;
+        found = true;
+        hit.t = t;
+        hit.inst = curInst;
+        hit.prim = prim;
+        hit.u = b1;
+        hit.v = b2;
+        hit.front = spt.front;
+      }
+    }
+  }
+  return SHADOW ? true : found;
+}
+
+}  // namespace sdb

@@ -1,0 +1,180 @@
+// Scene descriptors as the kernels see them. Filled on the host by the render
+// orchestration (render.cpp), uploaded once per render, read through the
+// __constant__ launch block (SdLaunch) by every kernel.
+//
+// Field meaning follows sundog's device/params.h (MaterialDesc 28-40,
+// LightDesc 42-71, EnvDesc 84-92, FlameDesc 97-105, CameraData 107-114); the
+// layouts are this library's own (pointers to device arrays, no OptiX or
+// texture-object handles: image lookups use the software filter in
+// sd_texture.cuh).
+#pragma once
+
+#include "sd_vec.h"
+
+namespace sdb {
+
+enum GeomKind : int { GK_SPHERE = 0, GK_RECT, GK_DISK, GK_CYLINDER, GK_PARABOLA, GK_MESH, GK_COUNT };
+enum TexKind : int { TX_SOLID = 0, TX_IMAGE, TX_CHECKER, TX_GRID };
+enum MatKind : int { MT_LAMBERT = 0, MT_METAL, MT_DIELECTRIC, MT_EMISSIVE, MT_WATER, MT_PLASTIC };
+enum LightKind : int { LT_RECT = 0, LT_DISK, LT_SPHERE, LT_POINT, LT_DISTANT, LT_MESH };
+enum BgKind : int { BG_SOLID = 0, BG_GRADIENT, BG_ENVMAP };
+
+constexpr uint16_t kMatNone = 0xFFFF;  // pass-through face
+
+struct SdTexture {
+  int kind;
+  float3 a, b;       // solid colour / checker + grid colours
+  float2 scale;      // checker / grid tiling
+  float width;       // grid line width (cell fraction)
+  int imgW, imgH;    // TX_IMAGE: texel grid
+  int srgb;          // TX_IMAGE: texels are sRGB-encoded
+  const uchar4* img; // TX_IMAGE: row-major RGBA8, row 0 = top of the image
+};
+
+struct SdMaterial {
+  int kind;
+  int texId;         // -1: use color
+  float3 color;
+  float roughness;   // GGX alpha = roughness^2; < 1e-3 is a delta lobe
+  float ior;
+  float intensity;   // emissive scale
+  int twoSided;      // emissive visible from both faces
+  float3 absorb;     // Beer-Lambert sigma inside (glass / water)
+  float waveAmp;     // water wave-normal strength
+  float waveFreq;    // water wave frequency (world xz)
+};
+
+struct SdLight {
+  int kind;
+  float3 p;          // centre / position
+  float3 u, v;       // rect / disk half-edge basis
+  float3 n;          // rect / disk front normal
+  float3 L;          // radiance (area, distant) or intensity (point)
+  float radius;
+  float area;        // rect / disk / mesh world area
+  float3 dir;        // distant: direction of travel
+  int twoSided;
+  int texId;
+  int flameId;       // owning flame (embedded lights), -1 = none
+  // LT_MESH: world-space triangle soup sampled by area.
+  const float3* mPos;
+  const uint3* mIdx;
+  const float2* mUv;
+  const float* mCdf; // mNumTris + 1 entries, [0] = 0, [n] = 1
+  int mNumTris;
+  float mNgSign;
+};
+
+struct SdEnv {
+  const float4* texels;  // width x height, row 0 = zenith
+  const float* margCdf;  // height + 1
+  const float* condCdf;  // height x (width + 1)
+  int width, height;
+  float rotate;          // radians about +Y
+  float intensity;
+  int importance;        // 0: uniform-sphere NEE
+};
+
+struct SdFlame {
+  float3 base;
+  float height, radius, intensity, sigma, noiseScale;
+  unsigned seed;
+  int steps;             // ray-march steps (reference: 32)
+};
+
+struct SdCamera {
+  float3 origin, lowerLeft, horizontal, vertical, u, v, w;
+  float lensRadius;
+};
+
+// Instance of a quadric or a mesh BLAS. w2o maps world to object space; its
+// transpose maps object-space normals to world space (inverse transpose).
+struct SdInstance {
+  float4 w2o[3];
+  int kind;          // GeomKind
+  int mesh;          // GK_MESH: mesh index
+  uint32_t mats;     // matFront | matBack << 16
+  int lightId;       // NEE light registered for this object, -1 = none
+  int cutoutTex;     // alpha-cutout texture, -1 = none
+  int flags;         // kInstMasked | kInstTransmissive
+  int pad0, pad1;
+};
+constexpr int kInstMasked = 1;        // a face is pass-through, or a cutout
+constexpr int kInstTransmissive = 2;  // a face is glass or water
+
+struct SdMesh {
+  const uint3* idx;
+  const float3* pos;
+  const float3* nrm;   // null: geometric normal
+  const float2* uv;    // null: barycentric uv
+  int root;            // first node of this mesh's BLAS in SdLaunch::nodes
+  int numTris;
+};
+
+// Binary BVH node: both children's boxes in one 64-byte node so a visit is
+// four 16-byte loads. child >= 0 is an inner node index; child < 0 is a leaf
+// whose primitives start at ~child, count in cnt.
+struct __align__(16) BvhNode {
+  float4 xy0;   // c0 lo.x hi.x lo.y hi.y
+  float4 xy1;   // c1 lo.x hi.x lo.y hi.y
+  float4 zz;    // c0 lo.z hi.z, c1 lo.z hi.z
+  int4 link;    // child0, child1, cnt0, cnt1
+};
+
+// Everything a launch needs, in constant memory.
+struct SdLaunch {
+  int width, height;
+  int sppTotal;
+  int sampleOffset;      // first sample index of this launch
+  int sppThisLaunch;
+  int maxDepth;
+  int nStrata;
+  float clampVal;
+  unsigned seed;
+  int transparentShadows;
+  int aovOn;
+
+  // work decomposition: path p -> (sample p / npixPad, tile-ordered pixel)
+  int tilesX;
+  int npixPad;
+  unsigned long long numPaths;
+  unsigned long long* pathCounter;
+  unsigned long long* rayCounter;
+
+  float4* sampleL;       // [sppThisLaunch][npixPad] radiance per sample
+  float4* sampleAlb;     // [sppThisLaunch][npixPad] first-hit albedo
+  float4* sampleNrm;     // [sppThisLaunch][npixPad] first-hit normal (camera)
+  float4* accum;         // film running means [height*width]
+  float4* aovAlbedo;
+  float4* aovNormal;
+
+  SdCamera cam;
+  int bgKind;
+  float3 bgA, bgB;
+  SdEnv env;
+
+  const SdTexture* textures;
+  const SdMaterial* materials;
+  const SdLight* lights;
+  int numLights;
+  const SdFlame* flames;
+  int numFlames;
+
+  const BvhNode* nodes;
+  const float4* tris;     // 3 float4 per leaf-ordered triangle; .w of the
+                          // first holds the mesh-local triangle index
+  const SdInstance* inst;
+  const SdMesh* meshes;
+  int tlasRoot;
+  int numInstances;
+
+  // learned path guiding (optional)
+  int guiding;
+  const void* guideNet;
+  float guideMix;
+  float* guideTrain;
+  unsigned long long* guideTrainCount;
+  unsigned long long guideTrainCap;
+};
+
+}  // namespace sdb
