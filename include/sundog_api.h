@@ -193,7 +193,8 @@ typedef struct {
   int32_t repeat;        /* >1: re-render the film this many times and report
                             the fastest render loop (timing aid); 0/1 = once */
   int32_t guiding;       /* 1 = learned path guiding (see sundog_guiding_*) */
-  int32_t reserved;
+  int32_t sample_offset; /* first sample index: the render folds samples
+                            [sample_offset, sample_offset + spp) */
 } sundog_render_ext;
 
 typedef struct {
@@ -236,6 +237,22 @@ SUNDOG_API int sundog_session_read(sundog_session*, float* film_rgba, float* aov
                                    float* aov_normal);
 SUNDOG_API int sundog_session_info(sundog_session*, sundog_session_stats*);
 SUNDOG_API void sundog_session_destroy(sundog_session*);
+
+/* Traversal visit counts over one full render of the session (a counting
+ * build of the path kernel, for the roofline's algorithmic bytes; never the
+ * timed path). Leaves the film holding that render. */
+typedef struct {
+  uint64_t rays;          /* radiance + shadow traces */
+  uint64_t box_tests;     /* child-box slab tests (2 per binary node visit) */
+  uint64_t tri_tests;     /* ray/triangle tests */
+  uint64_t quadric_tests; /* analytic quadric instance tests */
+  uint64_t blas_entries;  /* mesh instances entered (object-space rays) */
+} sundog_trace_counts;
+SUNDOG_API int sundog_session_trace_counts(sundog_session*, sundog_trace_counts*);
+
+/* Host<->device bytes moved by the library since load (uploads, downloads);
+ * bench.py reads the per-step difference for its end-to-end record. */
+SUNDOG_API void sundog_transfer_bytes(uint64_t* h2d, uint64_t* d2h);
 
 /* Derived scene state as JSON (lights after NEE registration, object
  * transforms, materials, flames, settings). Writes at most cap bytes including

@@ -54,7 +54,7 @@ class RenderExt(ctypes.Structure):
     _fields_ = [("film_rgba", ctypes.c_void_p), ("aov_albedo", ctypes.c_void_p),
                 ("aov_normal", ctypes.c_void_p), ("chunk_spp", ctypes.c_int32),
                 ("repeat", ctypes.c_int32), ("guiding", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("sample_offset", ctypes.c_int32)]
 
 
 class RenderResult(ctypes.Structure):
@@ -76,6 +76,12 @@ class SessionStats(ctypes.Structure):
                 ("setup_ms", ctypes.c_double)]
 
 
+class TraceCounts(ctypes.Structure):
+    _fields_ = [("rays", ctypes.c_uint64), ("box_tests", ctypes.c_uint64),
+                ("tri_tests", ctypes.c_uint64), ("quadric_tests", ctypes.c_uint64),
+                ("blas_entries", ctypes.c_uint64)]
+
+
 # Every symbol include/sundog_api.h declares (the first 27 are the drop-in
 # surface of the reference ABI).
 DROP_IN_SYMBOLS = [
@@ -95,6 +101,7 @@ ADDITIVE_SYMBOLS = [
     "sundog_set_flame_steps", "sundog_render_ex", "sundog_scene_debug_json",
     "sundog_selftest", "sundog_session_create", "sundog_session_render",
     "sundog_session_read", "sundog_session_info", "sundog_session_destroy",
+    "sundog_session_trace_counts", "sundog_transfer_bytes",
 ]
 
 _lib = None
@@ -155,6 +162,9 @@ def load(path=None):
     lib.sundog_session_render.argtypes = [vp, vp, ip, ctypes.POINTER(RenderResult)]
     lib.sundog_session_read.argtypes = [vp, vp, vp, vp]
     lib.sundog_session_info.argtypes = [vp, ctypes.POINTER(SessionStats)]
+    lib.sundog_session_trace_counts.argtypes = [vp, ctypes.POINTER(TraceCounts)]
+    lib.sundog_transfer_bytes.argtypes = [ctypes.POINTER(ctypes.c_uint64)] * 2
+    lib.sundog_transfer_bytes.restype = None
     lib.sundog_session_destroy.argtypes = [vp]
     lib.sundog_session_destroy.restype = None
     if path is None:

@@ -39,12 +39,13 @@ __device__ __forceinline__ float3 background(const SdLaunch& lp, float3 dir) {
 }
 
 // Straight-line transmittance toward a light (device/programs.cu:70-85).
+template <bool COUNT>
 __device__ __forceinline__ float3 shadowTransmittance(const SdLaunch& lp, float3 o, float3 d,
-                                                      float tmax) {
+                                                      float tmax, TraceCount* cnt) {
   TraceHit dummy;
   float trProd = 1.0f;
   float3 tau = v3(0.0f);
-  if (!traverse<true>(lp, o, d, tmax, dummy, trProd, tau)) return v3(0.0f);
+  if (!traverse<true, COUNT>(lp, o, d, tmax, dummy, trProd, tau, cnt)) return v3(0.0f);
   tau = v3(fmaxf(0.0f, tau.x), fmaxf(0.0f, tau.y), fmaxf(0.0f, tau.z));
   float3 tr = v3(trProd);
   if (hmax(tau) > 0.0f) tr = tr * vexp(-tau);
@@ -130,14 +131,16 @@ __device__ __forceinline__ void writeAov(const SdLaunch& lp, const Path& p, floa
 // One segment of the path: trace, media, surface or escape, NEE, BSDF
 // sample, roulette. Returns false when the path has ended.
 // (device/programs.cu:374-558)
-__device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned long long& rays) {
+template <bool COUNT>
+__device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned long long& rays,
+                                       TraceCount* cnt) {
   const bool hasEnv = lp.bgKind == BG_ENVMAP;
   const int nStrat = lp.numLights + (hasEnv ? 1 : 0);
 
   TraceHit h;
   float dummyTr = 1.0f;
   float3 dummyTau = v3(0.0f);
-  bool hit = traverse<false>(lp, p.o, p.d, 1e16f, h, dummyTr, dummyTau);
+  bool hit = traverse<false, COUNT>(lp, p.o, p.d, 1e16f, h, dummyTr, dummyTau, cnt);
   rays++;
 
   if (p.medDepth > 0) {
@@ -214,7 +217,7 @@ __device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned lon
       rays++;
       float3 so = nudge(x, transmitNee ? -ns : ns);
       float tmaxS = ls.dist * 0.999f;
-      float3 tr = shadowTransmittance(lp, so, ls.wi, tmaxS);
+      float3 tr = shadowTransmittance<COUNT>(lp, so, ls.wi, tmaxS, cnt);
       if (hmax(tr) > 0.0f) {
         if (lp.numFlames > 0 && lp.transparentShadows) {
           int skip = k < lp.numLights ? lp.lights[k].flameId : -1;
@@ -272,8 +275,10 @@ __device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned lon
   return p.depth < lp.maxDepth;
 }
 
-__global__ void __launch_bounds__(kRenderBlock) ptPersistent() {
+template <bool COUNT>
+__global__ void __launch_bounds__(kRenderBlock) ptPersistent(TraceCount* counts) {
   const SdLaunch& lp = c_lp;
+  TraceCount cnt = {0, 0, 0, 0};
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned ltMask = (1u << lane) - 1u;
@@ -305,7 +310,7 @@ __global__ void __launch_bounds__(kRenderBlock) ptPersistent() {
       continue;
     }
     if (active) {
-      if (!bounce(lp, p, rays)) {
+      if (!bounce<COUNT>(lp, p, rays, &cnt)) {
         float3 L = sanitize3(p.L);
         lp.sampleL[p.slot] = make_float4(L.x, L.y, L.z, 1.0f);
         active = false;
@@ -315,6 +320,12 @@ __global__ void __launch_bounds__(kRenderBlock) ptPersistent() {
   // One ray-counter update per warp.
   for (int off = 16; off > 0; off >>= 1) rays += __shfl_down_sync(full, rays, off);
   if (lane == 0 && rays) atomicAdd(lp.rayCounter, rays);
+  if (COUNT) {
+    atomicAdd(&counts->boxTests, cnt.boxTests);
+    atomicAdd(&counts->triTests, cnt.triTests);
+    atomicAdd(&counts->quadTests, cnt.quadTests);
+    atomicAdd(&counts->blasEntries, cnt.blasEntries);
+  }
 }
 
 // Running mean of this launch's samples into the film, in sample order.
@@ -354,13 +365,18 @@ int renderGridSize() {
   int dev = 0, sms = 0, perSm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, ptPersistent, kRenderBlock, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, ptPersistent<false>, kRenderBlock, 0);
   if (perSm < 1) perSm = 1;
   return sms * perSm;
 }
 
 cudaError_t launchRender(cudaStream_t st, int grid) {
-  ptPersistent<<<grid, kRenderBlock, 0, st>>>();
+  ptPersistent<false><<<grid, kRenderBlock, 0, st>>>(nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launchRenderCounting(cudaStream_t st, int grid, TraceCount* counts) {
+  ptPersistent<true><<<grid, kRenderBlock, 0, st>>>(counts);
   return cudaGetLastError();
 }
 

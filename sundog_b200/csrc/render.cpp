@@ -8,6 +8,7 @@
 // uploads. Each session_render then runs the sample loop on the device:
 // per chunk one persistent path-tracing launch plus one film fold.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -45,9 +46,12 @@ void DevBuf::alloc(size_t n) {
   cudaCheck(cudaMalloc(&ptr, n), "cudaMalloc");
   bytes = n;
 }
+std::atomic<unsigned long long> g_h2dBytes{0}, g_d2hBytes{0};
+
 void DevBuf::upload(const void* src, size_t n) {
   alloc(n);
   if (n) cudaCheck(cudaMemcpy(ptr, src, n, cudaMemcpyHostToDevice), "upload");
+  g_h2dBytes += n;
 }
 void DevBuf::release() {
   if (ptr) cudaFree(ptr);
@@ -148,6 +152,8 @@ RenderSession::~RenderSession() {
   if (stream) cudaStreamDestroy(stream);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  if (kev[0]) cudaEventDestroy(kev[0]);
+  if (kev[1]) cudaEventDestroy(kev[1]);
 }
 
 void RenderSession::build(const sundog_scene* h, const sundog_render_options* opt,
@@ -185,6 +191,8 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
   cudaCheck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
   cudaCheck(cudaEventCreate(&ev0), "event");
   cudaCheck(cudaEventCreate(&ev1), "event");
+  cudaCheck(cudaEventCreate(&kev[0]), "event");
+  cudaCheck(cudaEventCreate(&kev[1]), "event");
 
   // ---- assets ----
   auto tLoad = Clock::now();
@@ -383,6 +391,7 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
     chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)rs.spp, cap / perSample));
   }
   chunk = std::min(chunk, rs.spp);
+  sampleBase = ext && ext->sample_offset > 0 ? ext->sample_offset : 0;
   sampleL.alloc(npix * chunk * sizeof(float4));
   if (aov) {
     sampleAlb.alloc(npix * chunk * sizeof(float4));
@@ -451,14 +460,21 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
   cudaCheck(cudaEventRecord(ev0, st), "event");
   uint64_t launches = 0;
   int done = 0;
+  float kms = 0.0f;
   while (done < lp.sppTotal) {
     int n = std::min(chunk, lp.sppTotal - done);
-    lp.sampleOffset = done;
+    lp.sampleOffset = sampleBase + done;
     lp.sppThisLaunch = n;
     lp.numPaths = (unsigned long long)lp.npixPad * n;
     cudaCheck(cudaMemsetAsync(lp.pathCounter, 0, sizeof(unsigned long long), st), "counter reset");
     cudaCheck(setLaunch(lp, st), "launch params");
+    cudaCheck(cudaEventRecord(kev[0], st), "event");
     cudaCheck(launchRender(st, grid), "path kernel launch");
+    cudaCheck(cudaEventRecord(kev[1], st), "event");
+    cudaCheck(cudaEventSynchronize(kev[1]), "path kernel");
+    float one = 0.0f;
+    cudaCheck(cudaEventElapsedTime(&one, kev[0], kev[1]), "event time");
+    kms += one;
     cudaCheck(launchFold((int)npix, st), "fold launch");
     launches += 2;
     done += n;
@@ -482,13 +498,44 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
     res->mrays_per_sec = wall > 0 ? rays / wall / 1000.0 : 0.0;
     res->samples_per_sec = wall > 0 ? (double)npix * lp.sppTotal / (wall / 1000.0) : 0.0;
     res->kernel_launches = launches;
-    res->kernel_ms = evMs;
+    res->kernel_ms = kms;
   }
+}
+
+void RenderSession::countTraversal(sundog_trace_counts* out) {
+  DevBuf dc;
+  dc.alloc(sizeof(unsigned long long) * 4);
+  cudaCheck(cudaMemset(dc.ptr, 0, dc.bytes), "counter reset");
+  cudaCheck(cudaMemsetAsync(accum.ptr, 0, accum.bytes, stream), "film reset");
+  cudaCheck(cudaMemsetAsync(lp.rayCounter, 0, sizeof(unsigned long long), stream), "counter reset");
+  int done = 0;
+  size_t npix = (size_t)lp.width * lp.height;
+  while (done < lp.sppTotal) {
+    int n = std::min(chunk, lp.sppTotal - done);
+    lp.sampleOffset = sampleBase + done;
+    lp.sppThisLaunch = n;
+    lp.numPaths = (unsigned long long)lp.npixPad * n;
+    cudaCheck(cudaMemsetAsync(lp.pathCounter, 0, sizeof(unsigned long long), stream), "counter reset");
+    cudaCheck(setLaunch(lp, stream), "launch params");
+    cudaCheck(launchRenderCounting(stream, grid, (TraceCount*)dc.ptr), "counting launch");
+    cudaCheck(launchFold((int)npix, stream), "fold launch");
+    done += n;
+  }
+  cudaCheck(cudaStreamSynchronize(stream), "counting render");
+  unsigned long long c[4], rays = 0;
+  cudaCheck(cudaMemcpy(c, dc.ptr, sizeof c, cudaMemcpyDeviceToHost), "counts");
+  cudaCheck(cudaMemcpy(&rays, lp.rayCounter, sizeof rays, cudaMemcpyDeviceToHost), "ray count");
+  out->rays = rays;
+  out->box_tests = c[0];
+  out->tri_tests = c[1];
+  out->quadric_tests = c[2];
+  out->blas_entries = c[3];
 }
 
 void RenderSession::read(float* film, float* alb, float* nrm) {
   size_t n = (size_t)lp.width * lp.height * sizeof(float4);
   if (film) cudaCheck(cudaMemcpy(film, accum.ptr, n, cudaMemcpyDeviceToHost), "film download");
+  g_d2hBytes += (film ? n : 0) + (alb ? n : 0) + (nrm ? n : 0);
   if (alb) {
     if (!aov) throw std::runtime_error("session: AOVs were not requested");
     cudaCheck(cudaMemcpy(alb, aovAlb.ptr, n, cudaMemcpyDeviceToHost), "aov download");
@@ -590,6 +637,19 @@ extern "C" int sundog_session_info(sundog_session* sh, sundog_session_stats* st)
   st->setup_ms = s->setupMs;
   return SUNDOG_OK;
   SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_session_trace_counts(sundog_session* sh, sundog_trace_counts* out) {
+  SDB_TRY
+  if (!sh || !out) throw std::runtime_error("session: null argument");
+  reinterpret_cast<RenderSession*>(sh)->countTraversal(out);
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" void sundog_transfer_bytes(uint64_t* h2d, uint64_t* d2h) {
+  if (h2d) *h2d = g_h2dBytes.load();
+  if (d2h) *d2h = g_d2hBytes.load();
 }
 
 extern "C" void sundog_session_destroy(sundog_session* sh) {

@@ -45,6 +45,7 @@ struct RenderSession {
   bool quiet = false;
   bool aov = false;
   int chunk = 1;
+  int sampleBase = 0;  // first sample index of a render
   int grid = 0;
   size_t freeBefore = 0, deviceBytes = 0;
   size_t meshTriangles = 0, numNodes = 0, numTris = 0;
@@ -54,6 +55,7 @@ struct RenderSession {
   double lastRenderMs = 0, lastKernelMs = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t kev[2] = {nullptr, nullptr};  // around each path-kernel launch
 
   DevBuf envTex, envMarg, envCond;
   std::vector<DevBuf> texImages;
@@ -66,6 +68,7 @@ struct RenderSession {
   void build(const sundog_scene* h, const sundog_render_options* opt, const sundog_render_ext* ext);
   void render(cudaStream_t st, bool reset, sundog_render_result* res);
   void read(float* film, float* alb, float* nrm);
+  void countTraversal(sundog_trace_counts* out);
 };
 
 }  // namespace sdb

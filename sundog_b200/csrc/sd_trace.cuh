@@ -37,6 +37,12 @@ struct TraceHit {
   bool front;
 };
 
+// Visit counts of the traversal, gathered only by the counting variant of the
+// path kernel (for the algorithmic-bytes roofline), never in timed launches.
+struct TraceCount {
+  unsigned long long boxTests, triTests, quadTests, blasEntries;
+};
+
 struct ShadePt {
   float3 nFront;  // world unit normal of the canonical front side
   float u, v;
@@ -238,9 +244,10 @@ __device__ __forceinline__ bool shadowCross(const SdLaunch& lp, const ShadePt& s
 // SHADOW = false: closest accepted hit, returns whether one was found.
 // SHADOW = true: returns false when occluded, else accumulates the
 // transparent-crossing terms into trProd / tau.
-template <bool SHADOW>
+template <bool SHADOW, bool COUNT = false>
 __device__ __forceinline__ bool traverse(const SdLaunch& lp, float3 O, float3 D, float tmax,
-                                         TraceHit& hit, float& trProd, float3& tau) {
+                                         TraceHit& hit, float& trProd, float3& tau,
+                                         TraceCount* cnt = nullptr) {
   if (lp.numInstances == 0) return SHADOW;
   int stack[kStackSize];
   int sp = 0;
@@ -259,6 +266,7 @@ __device__ __forceinline__ bool traverse(const SdLaunch& lp, float3 O, float3 D,
   while (true) {
     if (cur >= 0) {
       BvhNode nd = loadNode(nodes, cur);
+      if (COUNT) cnt->boxTests += 2;
       float ta, tb;
       bool ha, hb;
       boxPair(nd, oi, id, tmin, tmax, ta, tb, ha, hb);
@@ -302,6 +310,7 @@ __device__ __forceinline__ bool traverse(const SdLaunch& lp, float3 O, float3 D,
       const SdInstance& in = lp.inst[start];
       float3 o2 = xfPoint(in.w2o, O), d2 = xfVec(in.w2o, D);
       if (in.kind == GK_MESH) {
+        if (COUNT) cnt->blasEntries++;
         if (sp < kStackSize) {
           stack[sp++] = kToTlas;
           inBlas = true;
@@ -315,6 +324,7 @@ __device__ __forceinline__ bool traverse(const SdLaunch& lp, float3 O, float3 D,
         }
         continue;
       }
+      if (COUNT) cnt->quadTests++;
       QHits qh = hitQuadric(in.kind, o2, d2, tmin, tmax);
       for (int k = 0; k < qh.n; k++) {
         const QHit& q = qh.h[k];
@@ -344,6 +354,7 @@ __device__ __forceinline__ bool traverse(const SdLaunch& lp, float3 O, float3 D,
     for (int k = 0; k < count; k++) {
       const float4* tp = lp.tris + 3 * (size_t)(start + k);
       float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+      if (COUNT) cnt->triTests++;
       float t, b1, b2;
       float3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
       if (!wtHit(wr, ro, p0, p1, p2, tmin, tmax, t, b1, b2)) continue;

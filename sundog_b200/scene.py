@@ -317,14 +317,15 @@ class Scene(object):
 class Session(object):
     """A scene resident on the device (sundog_session_*)."""
 
-    def __init__(self, scene, base_dir=".", aov=False, chunk_spp=0, guiding=0, **opts):
+    def __init__(self, scene, base_dir=".", aov=False, chunk_spp=0, guiding=0, sample_offset=0,
+                 **opts):
         self.lib = abi.load()
         h = scene.build(base_dir, self.lib)
         try:
             o = abi.options(**opts)
             dummy = np.zeros(4, np.float32)
             ext = abi.RenderExt(None, dummy.ctypes.data if aov else None, None, chunk_spp, 1,
-                                guiding, 0)
+                                guiding, sample_offset)
             self.handle = self.lib.sundog_session_create(h, ctypes.byref(o), ctypes.byref(ext))
             if not self.handle:
                 raise abi.SundogError("session: " + abi.last_error(self.lib))
@@ -336,6 +337,7 @@ class Session(object):
                   self.lib)
 
     def render(self, stream=None, reset=True):
+        """One full render on `stream` (a cudaStream_t as int; None = own)."""
         res = abi.RenderResult()
         abi.check(self.lib.sundog_session_render(self.handle, stream, 1 if reset else 0,
                                                  ctypes.byref(res)), "session render", self.lib)
