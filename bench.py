@@ -303,6 +303,9 @@ def run_ours(args):
                                        "tri_tests": counts.tri_tests / counts.rays,
                                        "quadric_tests": counts.quadric_tests / counts.rays,
                                        "blas_entries": counts.blas_entries / counts.rays},
+                    "simt": {"traversal_lanes_per_iter": counts.trav_lanes / max(counts.trav_iters, 1),
+                             "path_loop_lanes_per_iter": counts.loop_lanes / max(counts.loop_iters, 1),
+                             "traversal_iters_per_ray": 32.0 * counts.trav_iters / max(counts.rays, 1)},
                     "note": "algorithmic bytes on a binary BVH (32 B/box, 36 B/tri, 48 B/"
                             "quadric, 64 B/instance) per path-kernel launch over its CUDA-event "
                             "duration; the BVH (<4 MB) and env tables are L2-resident, so HBM "

@@ -247,6 +247,10 @@ typedef struct {
   uint64_t tri_tests;     /* ray/triangle tests */
   uint64_t quadric_tests; /* analytic quadric instance tests */
   uint64_t blas_entries;  /* mesh instances entered (object-space rays) */
+  uint64_t trav_iters;    /* warp iterations of the traversal loop */
+  uint64_t trav_lanes;    /* active lanes summed over those iterations */
+  uint64_t loop_iters;    /* warp iterations of the path loop */
+  uint64_t loop_lanes;    /* lanes running a path segment in them */
 } sundog_trace_counts;
 SUNDOG_API int sundog_session_trace_counts(sundog_session*, sundog_trace_counts*);
 

@@ -9,7 +9,7 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libsundog.so")
+LIB_PATH = os.environ.get("SUNDOG_B200_LIB") or os.path.join(HERE, "lib", "libsundog.so")
 
 c_d3 = ctypes.c_double * 3
 
@@ -79,7 +79,9 @@ class SessionStats(ctypes.Structure):
 class TraceCounts(ctypes.Structure):
     _fields_ = [("rays", ctypes.c_uint64), ("box_tests", ctypes.c_uint64),
                 ("tri_tests", ctypes.c_uint64), ("quadric_tests", ctypes.c_uint64),
-                ("blas_entries", ctypes.c_uint64)]
+                ("blas_entries", ctypes.c_uint64), ("trav_iters", ctypes.c_uint64),
+                ("trav_lanes", ctypes.c_uint64), ("loop_iters", ctypes.c_uint64),
+                ("loop_lanes", ctypes.c_uint64)]
 
 
 # Every symbol include/sundog_api.h declares (the first 27 are the drop-in

@@ -66,16 +66,19 @@ def _run(cmd, verbose):
     return r.stdout
 
 
-def build(verbose=False, force=False):
-    """Compile every translation unit (cached by content hash) and link."""
-    os.makedirs(OUT_DIR, exist_ok=True)
+def build(verbose=False, force=False, defines=(), out=None):
+    """Compile every translation unit (cached by content hash) and link.
+    `defines` adds -D flags to the CUDA units (kernel tuning experiments);
+    `out` overrides the output library path."""
+    lib_path = out or LIB
+    os.makedirs(os.path.dirname(lib_path), exist_ok=True)
     os.makedirs(OBJ_DIR, exist_ok=True)
     hdr = _headers_digest()
     objs = []
     for src in _sources():
         path = os.path.join(CSRC, src)
         is_cu = src.endswith(".cu")
-        flags = NVCC_FLAGS if is_cu else CXX_FLAGS
+        flags = (NVCC_FLAGS + ["-D" + d for d in defines]) if is_cu else CXX_FLAGS
         tag = _digest(path, flags + [hdr])
         obj = os.path.join(OBJ_DIR, "%s.%s.o" % (src, tag))
         if force or not os.path.exists(obj):
@@ -87,10 +90,10 @@ def build(verbose=False, force=False):
             if verbose and out.strip():
                 print(out)
         objs.append(obj)
-    link = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static",
+    link = [NVCC] + ARCH + ["-shared", "-o", lib_path] + objs + ["-cudart", "static",
                                                                "-Xlinker", "-soname=libsundog.so"]
     _run(link, verbose)
-    return LIB
+    return lib_path
 
 
 if __name__ == "__main__":

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstring>
 
 namespace sdb {
 
@@ -184,6 +185,236 @@ BvhBuild buildBvh(const std::vector<Box3>& boxes, int maxLeaf, int nodeBase, int
   }
   bd.out.order = bd.ids;
   return bd.out;
+}
+
+}  // namespace sdb
+
+// ---- explicit binary tree + 8-wide collapse ------------------------------------
+
+namespace sdb {
+
+namespace {
+
+struct BinBuilder {
+  Builder core;
+  BinTree out;
+  BinBuilder(const std::vector<Box3>& b, int ml) : core(b, ml, 0, 0) {}
+
+  int build(int b, int e, int depth) {
+    out.maxDepth = std::max(out.maxDepth, depth);
+    int idx = (int)out.nodes.size();
+    out.nodes.push_back(BinNode{});
+    out.nodes[idx].box = core.rangeBox(b, e);
+    int m = core.split(b, e, depth);
+    if (m < 0) {
+      out.nodes[idx].start = b;
+      out.nodes[idx].count = e - b;
+      return idx;
+    }
+    int l = build(b, m, depth + 1);
+    int r = build(m, e, depth + 1);
+    out.nodes[idx].left = l;
+    out.nodes[idx].right = r;
+    return idx;
+  }
+};
+
+inline int exponentFor(float lo, float hi) {
+  double ext = (double)hi - (double)lo;
+  if (!(ext > 0.0)) return -120;
+  int e = (int)std::ceil(std::log2(ext / 255.0));
+  if (ext / std::ldexp(1.0, e) > 255.0) e++;
+  return std::min(std::max(e, -120), 120);
+}
+
+inline uint8_t byteOf(const float4& v, int k) {
+  uint32_t w[4];
+  std::memcpy(w, &v, 16);
+  return (uint8_t)(w[k >> 2] >> (8 * (k & 3)));
+}
+inline void setByte(float4& v, int k, uint8_t b) {
+  uint32_t w[4];
+  std::memcpy(w, &v, 16);
+  w[k >> 2] = (w[k >> 2] & ~(0xFFu << (8 * (k & 3)))) | ((uint32_t)b << (8 * (k & 3)));
+  std::memcpy(&v, w, 16);
+}
+inline uint32_t wordOf(const float4& v, int k) {
+  uint32_t w[4];
+  std::memcpy(w, &v, 16);
+  return w[k];
+}
+inline void setWord(float4& v, int k, uint32_t x) {
+  uint32_t w[4];
+  std::memcpy(w, &v, 16);
+  w[k] = x;
+  std::memcpy(&v, w, 16);
+}
+
+// Quantised coordinate of one bound, rounded outward and verified against
+// the float decode the traversal performs (p + q * 2^e).
+uint8_t quantLo(float p, int e, float v) {
+  double s = std::ldexp(1.0, e);
+  long q = (long)std::floor(((double)v - (double)p) / s);
+  q = std::min(std::max(q, 0L), 255L);
+  while (q > 0 && (float)(p + (float)((double)q * s)) > v) q--;
+  return (uint8_t)q;
+}
+uint8_t quantHi(float p, int e, float v) {
+  double s = std::ldexp(1.0, e);
+  long q = (long)std::ceil(((double)v - (double)p) / s);
+  q = std::min(std::max(q, 0L), 255L);
+  while (q < 255 && (float)(p + (float)((double)q * s)) < v) q++;
+  return (uint8_t)q;
+}
+
+}  // namespace
+
+BinTree buildBinary(const std::vector<Box3>& boxes, int maxLeaf) {
+  BinBuilder bb(boxes, maxLeaf);
+  if (!boxes.empty()) bb.build(0, (int)boxes.size(), 0);
+  bb.out.order = bb.core.ids;
+  return bb.out;
+}
+
+Box3 cwChildBox(const CwNode& n, int s) {
+  float p[3] = {n.a.x, n.a.y, n.a.z};
+  uint32_t ew = wordOf(n.a, 3);
+  Box3 b;
+  float* lo = &b.lo.x;
+  float* hi = &b.hi.x;
+  const float4* qlo[3] = {&n.c, &n.c, &n.d};
+  const float4* qhi[3] = {&n.d, &n.e, &n.e};
+  const int qloOff[3] = {0, 8, 0}, qhiOff[3] = {8, 0, 8};
+  for (int a = 0; a < 3; a++) {
+    int e = (int)(int8_t)(ew >> (8 * a));
+    float sc = std::ldexp(1.0f, e);
+    lo[a] = p[a] + (float)byteOf(*qlo[a], qloOff[a] + s) * sc;
+    hi[a] = p[a] + (float)byteOf(*qhi[a], qhiOff[a] + s) * sc;
+  }
+  return b;
+}
+
+CwBuild buildCw(const std::vector<Box3>& boxes, int maxLeaf, int nodeBase, int primBase) {
+  CwBuild out;
+  int n = (int)boxes.size();
+  BinTree bt = buildBinary(boxes, std::min(std::max(maxLeaf, 1), kCwLeafMax));
+  if (n == 0) {
+    // No primitives: one node with no valid slot.
+    CwNode z;
+    std::memset(&z, 0, sizeof z);
+    out.nodes.push_back(z);
+    return out;
+  }
+  struct Job {
+    int bin;    // binary node collapsed into this wide node
+    int slot;   // index in out.nodes
+    int depth;
+  };
+  std::vector<Job> queue;
+  out.nodes.push_back(CwNode{});
+  queue.push_back({0, 0, 0});
+  const float3 dirs[8] = {v3(1, 1, 1),   v3(-1, 1, 1),  v3(1, -1, 1),  v3(-1, -1, 1),
+                          v3(1, 1, -1),  v3(-1, 1, -1), v3(1, -1, -1), v3(-1, -1, -1)};
+  for (size_t qi = 0; qi < queue.size(); qi++) {
+    Job job = queue[qi];
+    out.maxDepth = std::max(out.maxDepth, job.depth);
+    // Gather up to 8 children by repeatedly opening the largest internal one.
+    std::vector<int> kids;
+    const BinNode& root = bt.nodes[job.bin];
+    if (root.left < 0) {
+      kids.push_back(job.bin);  // a leaf at the top: one leaf slot
+    } else {
+      kids.push_back(root.left);
+      kids.push_back(root.right);
+      while (kids.size() < 8) {
+        int best = -1;
+        float bestA = -1.0f;
+        for (size_t k = 0; k < kids.size(); k++) {
+          const BinNode& c = bt.nodes[kids[k]];
+          if (c.left < 0) continue;
+          float3 e = c.box.hi - c.box.lo;
+          float a = e.x * e.y + e.y * e.z + e.z * e.x;
+          if (a > bestA) {
+            bestA = a;
+            best = (int)k;
+          }
+        }
+        if (best < 0) break;
+        int b = kids[best];
+        kids.erase(kids.begin() + best);
+        kids.push_back(bt.nodes[b].left);
+        kids.push_back(bt.nodes[b].right);
+      }
+    }
+    // Slot assignment: greedy auction on the alignment of each child's
+    // offset from the node centre with the slot's octant diagonal.
+    Box3 nb = boxEmpty();
+    for (int k : kids) boxGrow(nb, bt.nodes[k].box);
+    float3 ctr = (nb.lo + nb.hi) * 0.5f;
+    struct Cand { float score; int kid, slot; };
+    std::vector<Cand> cands;
+    for (size_t k = 0; k < kids.size(); k++) {
+      const BinNode& c = bt.nodes[kids[k]];
+      float3 off = (c.box.lo + c.box.hi) * 0.5f - ctr;
+      for (int s = 0; s < 8; s++) cands.push_back({dot(off, dirs[s]), (int)k, s});
+    }
+    std::sort(cands.begin(), cands.end(), [](const Cand& x, const Cand& y) {
+      if (x.score != y.score) return x.score > y.score;
+      if (x.kid != y.kid) return x.kid < y.kid;
+      return x.slot < y.slot;
+    });
+    int slotKid[8];
+    bool kidUsed[8] = {false, false, false, false, false, false, false, false};
+    for (int s = 0; s < 8; s++) slotKid[s] = -1;
+    for (const Cand& c : cands) {
+      if (slotKid[c.slot] >= 0 || kidUsed[c.kid]) continue;
+      slotKid[c.slot] = c.kid;
+      kidUsed[c.kid] = true;
+    }
+    // Node header and quantisation grid.
+    CwNode nd;
+    std::memset(&nd, 0, sizeof nd);
+    int ex = exponentFor(nb.lo.x, nb.hi.x), ey = exponentFor(nb.lo.y, nb.hi.y),
+        ez = exponentFor(nb.lo.z, nb.hi.z);
+    nd.a = make_float4(nb.lo.x, nb.lo.y, nb.lo.z, 0.0f);
+    uint32_t imask = 0;
+    int internalCount = 0;
+    for (int s = 0; s < 8; s++)
+      if (slotKid[s] >= 0 && bt.nodes[kids[slotKid[s]]].left >= 0) internalCount++;
+    int childBase = (int)out.nodes.size();
+    out.nodes.resize(out.nodes.size() + internalCount);
+    int primBaseHere = (int)out.order.size();
+    int internalSeen = 0, primOff = 0;
+    for (int s = 0; s < 8; s++) {
+      if (slotKid[s] < 0) continue;
+      const BinNode& c = bt.nodes[kids[slotKid[s]]];
+      setByte(nd.c, s, quantLo(nb.lo.x, ex, c.box.lo.x));
+      setByte(nd.c, 8 + s, quantLo(nb.lo.y, ey, c.box.lo.y));
+      setByte(nd.d, s, quantLo(nb.lo.z, ez, c.box.lo.z));
+      setByte(nd.d, 8 + s, quantHi(nb.lo.x, ex, c.box.hi.x));
+      setByte(nd.e, s, quantHi(nb.lo.y, ey, c.box.hi.y));
+      setByte(nd.e, 8 + s, quantHi(nb.lo.z, ez, c.box.hi.z));
+      uint8_t meta;
+      if (c.left >= 0) {
+        imask |= 1u << s;
+        meta = 0xFF;
+        queue.push_back({kids[slotKid[s]], childBase + internalSeen, job.depth + 1});
+        internalSeen++;
+      } else {
+        meta = (uint8_t)((c.count << 5) | primOff);
+        for (int k = 0; k < c.count; k++) out.order.push_back(bt.order[c.start + k]);
+        primOff += c.count;
+      }
+      setByte(nd.b, 8 + s, meta);
+    }
+    uint32_t ew = (uint32_t)(uint8_t)(int8_t)ex | ((uint32_t)(uint8_t)(int8_t)ey << 8) |
+                  ((uint32_t)(uint8_t)(int8_t)ez << 16) | (imask << 24);
+    setWord(nd.a, 3, ew);
+    setWord(nd.b, 0, (uint32_t)(nodeBase + childBase));
+    setWord(nd.b, 1, (uint32_t)(primBase + primBaseHere));
+    out.nodes[job.slot] = nd;
+  }
+  return out;
 }
 
 }  // namespace sdb

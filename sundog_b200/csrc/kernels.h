@@ -7,10 +7,21 @@
 
 namespace sdb {
 
-constexpr int kRenderBlock = 128;
+#ifndef SDB_RENDER_BLOCK
+#define SDB_RENDER_BLOCK 128
+#endif
+// Resident 128-thread blocks per SM the path kernel is compiled for: 6 caps
+// it at 85 registers; the sweep in profiles/ measured 6 fastest (occupancy
+// beats the spills it costs).
+#ifndef SDB_MIN_BLOCKS
+#define SDB_MIN_BLOCKS 6
+#endif
+constexpr int kRenderBlock = SDB_RENDER_BLOCK;
 
 // Path tracer (pt_kernel.cu).
 cudaError_t setLaunch(const SdLaunch& lp, cudaStream_t st);
+// BVH layout the kernels were compiled for: 2 (BvhNode) or 8 (CwNode).
+int bvhWidth();
 int renderGridSize();
 cudaError_t launchRender(cudaStream_t st, int grid);
 cudaError_t launchFold(int npix, cudaStream_t st);

@@ -276,9 +276,9 @@ __device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned lon
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(kRenderBlock) ptPersistent(TraceCount* counts) {
+__global__ void __launch_bounds__(kRenderBlock, SDB_MIN_BLOCKS) ptPersistent(TraceCount* counts) {
   const SdLaunch& lp = c_lp;
-  TraceCount cnt = {0, 0, 0, 0};
+  TraceCount cnt = {0, 0, 0, 0, 0, 0, 0, 0};
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned ltMask = (1u << lane) - 1u;
@@ -310,6 +310,7 @@ __global__ void __launch_bounds__(kRenderBlock) ptPersistent(TraceCount* counts)
       continue;
     }
     if (active) {
+      if (COUNT) countWarp(&cnt, cnt.loopIters, cnt.loopLanes);
       if (!bounce<COUNT>(lp, p, rays, &cnt)) {
         float3 L = sanitize3(p.L);
         lp.sampleL[p.slot] = make_float4(L.x, L.y, L.z, 1.0f);
@@ -325,6 +326,10 @@ __global__ void __launch_bounds__(kRenderBlock) ptPersistent(TraceCount* counts)
     atomicAdd(&counts->triTests, cnt.triTests);
     atomicAdd(&counts->quadTests, cnt.quadTests);
     atomicAdd(&counts->blasEntries, cnt.blasEntries);
+    atomicAdd(&counts->travIters, cnt.travIters);
+    atomicAdd(&counts->travLanes, cnt.travLanes);
+    atomicAdd(&counts->loopIters, cnt.loopIters);
+    atomicAdd(&counts->loopLanes, cnt.loopLanes);
   }
 }
 
@@ -360,6 +365,8 @@ __global__ void ptFold() {
 cudaError_t setLaunch(const SdLaunch& lp, cudaStream_t st) {
   return cudaMemcpyToSymbolAsync(c_lp, &lp, sizeof(SdLaunch), 0, cudaMemcpyHostToDevice, st);
 }
+
+int bvhWidth() { return SDB_WIDE_BVH ? 8 : 2; }
 
 int renderGridSize() {
   int dev = 0, sms = 0, perSm = 0;

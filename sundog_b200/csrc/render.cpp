@@ -299,8 +299,8 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
                             o.xform.vec(v3(0, 0, 1)));
   }
 
-  // BLAS per mesh, TLAS over objects.
-  std::vector<BvhNode> allNodes;
+  // BLAS per mesh, TLAS over objects: compressed 8-wide trees in one array
+  // (TLAS first), triangles stored in leaf order.
   std::vector<float4> allTris;
   int nObj = (int)scene.objects.size();
   std::vector<Box3> instBoxes(nObj);
@@ -315,11 +315,28 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
       for (int c = 0; c < 8; c++)
         boxGrow(b, o.xform.point(v3(c & 1 ? hi.x : lo.x, c & 2 ? hi.y : lo.y, c & 4 ? hi.z : lo.z)));
     }
+    // World boxes come from rounded corner transforms: pad by a few ulps.
+    float3 pad = (vmax(vmax(b.hi, -b.hi), vmax(b.lo, -b.lo)) + v3(1.0f)) * 1e-6f;
+    b.lo = b.lo - pad;
+    b.hi = b.hi + pad;
     instBoxes[i] = b;
   }
-  BvhBuild tlas = buildBvh(instBoxes, 1, 0, 0);
-  allNodes = tlas.nodes;
-  tlasDepth = tlas.maxDepth;
+  // Kernel-matched layout: binary nodes, or compressed 8-wide nodes.
+  const bool wide = bvhWidth() == 8;
+  std::vector<CwNode> cwNodes;
+  std::vector<BvhNode> binNodes;
+  std::vector<int> tlasOrder;
+  if (wide) {
+    CwBuild tlas = buildCw(instBoxes, 1, 0, 0);
+    cwNodes = tlas.nodes;
+    tlasOrder = tlas.order;
+    tlasDepth = tlas.maxDepth;
+  } else {
+    BvhBuild tlas = buildBvh(instBoxes, 1, 0, 0);
+    binNodes = tlas.nodes;
+    tlasOrder = tlas.order;
+    tlasDepth = tlas.maxDepth;
+  }
   blasDepth = 0;
   for (size_t i = 0; i < meshes.size(); i++) {
     const HostMesh& m = meshes[i];
@@ -331,13 +348,24 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
       boxGrow(b, m.pos[m.idx[t].z]);
       tb[t] = b;
     }
-    int nodeBase = (int)allNodes.size();
     int primBase = (int)(allTris.size() / 3);
-    BvhBuild bl = buildBvh(tb, 4, nodeBase, primBase);
-    blasDepth = std::max(blasDepth, bl.maxDepth);
-    meshDescs[i].root = nodeBase;
-    allNodes.insert(allNodes.end(), bl.nodes.begin(), bl.nodes.end());
-    for (int k : bl.order) {
+    std::vector<int> order;
+    if (wide) {
+      int nodeBase = (int)cwNodes.size();
+      CwBuild bl = buildCw(tb, kCwLeafMax, nodeBase, primBase);
+      blasDepth = std::max(blasDepth, bl.maxDepth);
+      meshDescs[i].root = nodeBase;
+      cwNodes.insert(cwNodes.end(), bl.nodes.begin(), bl.nodes.end());
+      order = bl.order;
+    } else {
+      int nodeBase = (int)binNodes.size();
+      BvhBuild bl = buildBvh(tb, 4, nodeBase, primBase);
+      blasDepth = std::max(blasDepth, bl.maxDepth);
+      meshDescs[i].root = nodeBase;
+      binNodes.insert(binNodes.end(), bl.nodes.begin(), bl.nodes.end());
+      order = bl.order;
+    }
+    for (int k : order) {
       const uint3& t = m.idx[k];
       float3 a = m.pos[t.x], b = m.pos[t.y], c = m.pos[t.z];
       int ki = k;
@@ -348,10 +376,10 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
       allTris.push_back(make_float4(c.x, c.y, c.z, 0.0f));
     }
   }
-  // Instances in TLAS leaf order (leaf start = position in this array).
+  // Instances in TLAS leaf order (leaf primitive index = position here).
   std::vector<SdInstance> inst(nObj);
   for (int k = 0; k < nObj; k++) {
-    const ObjectCfg& o = scene.objects[tlas.order[k]];
+    const ObjectCfg& o = scene.objects[tlasOrder[k]];
     SdInstance& in = inst[k];
     std::memset(&in, 0, sizeof in);
     invertAffine(o.xform, in.w2o);
@@ -364,9 +392,12 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
     bool trans = matTransmissive(scene, o.matFront) || matTransmissive(scene, o.matBack);
     in.flags = (masked ? kInstMasked : 0) | (trans ? kInstTransmissive : 0);
   }
-  numNodes = allNodes.size();
+  numNodes = wide ? cwNodes.size() : binNodes.size();
   numTris = allTris.size() / 3;
-  dNodes.upload(allNodes.data(), allNodes.size() * sizeof(BvhNode));
+  if (wide)
+    dNodes.upload(cwNodes.data(), cwNodes.size() * sizeof(CwNode));
+  else
+    dNodes.upload(binNodes.data(), binNodes.size() * sizeof(BvhNode));
   dTris.upload(allTris.data(), allTris.size() * sizeof(float4));
   dInst.upload(inst.data(), inst.size() * sizeof(SdInstance));
   dMeshes.upload(meshDescs.data(), meshDescs.size() * sizeof(SdMesh));
@@ -432,7 +463,8 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
   l.numLights = (int)lights.size();
   l.flames = (const SdFlame*)dFlames.ptr;
   l.numFlames = (int)scene.flames.size();
-  l.nodes = (const BvhNode*)dNodes.ptr;
+  l.nodes = wide ? nullptr : (const BvhNode*)dNodes.ptr;
+  l.cw = wide ? (const CwNode*)dNodes.ptr : nullptr;
   l.tris = (const float4*)dTris.ptr;
   l.inst = (const SdInstance*)dInst.ptr;
   l.meshes = (const SdMesh*)dMeshes.ptr;
@@ -504,7 +536,7 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
 
 void RenderSession::countTraversal(sundog_trace_counts* out) {
   DevBuf dc;
-  dc.alloc(sizeof(unsigned long long) * 4);
+  dc.alloc(sizeof(unsigned long long) * 8);
   cudaCheck(cudaMemset(dc.ptr, 0, dc.bytes), "counter reset");
   cudaCheck(cudaMemsetAsync(accum.ptr, 0, accum.bytes, stream), "film reset");
   cudaCheck(cudaMemsetAsync(lp.rayCounter, 0, sizeof(unsigned long long), stream), "counter reset");
@@ -522,7 +554,7 @@ void RenderSession::countTraversal(sundog_trace_counts* out) {
     done += n;
   }
   cudaCheck(cudaStreamSynchronize(stream), "counting render");
-  unsigned long long c[4], rays = 0;
+  unsigned long long c[8], rays = 0;
   cudaCheck(cudaMemcpy(c, dc.ptr, sizeof c, cudaMemcpyDeviceToHost), "counts");
   cudaCheck(cudaMemcpy(&rays, lp.rayCounter, sizeof rays, cudaMemcpyDeviceToHost), "ray count");
   out->rays = rays;
@@ -530,6 +562,10 @@ void RenderSession::countTraversal(sundog_trace_counts* out) {
   out->tri_tests = c[1];
   out->quadric_tests = c[2];
   out->blas_entries = c[3];
+  out->trav_iters = c[4];
+  out->trav_lanes = c[5];
+  out->loop_iters = c[6];
+  out->loop_lanes = c[7];
 }
 
 void RenderSession::read(float* film, float* alb, float* nrm) {

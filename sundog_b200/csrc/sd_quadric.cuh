@@ -11,6 +11,17 @@
 
 #include "sd_types.h"
 
+// Paths most pixels never take (water normals, flame marches, quadric
+// roots) are compiled out of line in device code, keeping the hot loop's
+// instruction footprint small; host code inlines them as usual.
+#ifndef SDB_COLD
+#if defined(__CUDA_ARCH__)
+#define SDB_COLD static __host__ __device__ __noinline__
+#else
+#define SDB_COLD static inline
+#endif
+#endif
+
 namespace sdb {
 
 struct QHit {
@@ -147,7 +158,7 @@ SDB_HD QHits hitParabola(float3 o, float3 d, float tmin, float tmax) {
   return r;
 }
 
-SDB_HD QHits hitQuadric(int kind, float3 o, float3 d, float tmin, float tmax) {
+SDB_COLD QHits hitQuadric(int kind, float3 o, float3 d, float tmin, float tmax) {
   switch (kind) {
     case GK_SPHERE: return hitSphere(o, d, tmin, tmax);
     case GK_RECT: return hitRect(o, d, tmin, tmax);

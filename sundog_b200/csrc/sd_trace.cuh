@@ -18,6 +18,10 @@
 // Triangles use the watertight test of Woop, Benthin and Wald (JCGT 2013).
 #pragma once
 
+#ifndef SDB_WIDE_BVH
+#define SDB_WIDE_BVH 0
+#endif
+
 #include "sd_quadric.cuh"
 #include "sd_texture.cuh"
 #include "sd_types.h"
@@ -41,7 +45,19 @@ struct TraceHit {
 // path kernel (for the algorithmic-bytes roofline), never in timed launches.
 struct TraceCount {
   unsigned long long boxTests, triTests, quadTests, blasEntries;
+  // SIMT occupancy of the loops, summed by the first active lane of each
+  // warp: iterations executed, and active lanes over those iterations.
+  unsigned long long travIters, travLanes, loopIters, loopLanes;
 };
+
+__device__ __forceinline__ void countWarp(TraceCount* cnt, unsigned long long& iters,
+                                          unsigned long long& lanes) {
+  unsigned m = __activemask();
+  if ((threadIdx.x & 31) == (unsigned)(__ffs(m) - 1)) {
+    iters++;
+    lanes += __popc(m);
+  }
+}
 
 struct ShadePt {
   float3 nFront;  // world unit normal of the canonical front side
@@ -241,11 +257,263 @@ __device__ __forceinline__ bool shadowCross(const SdLaunch& lp, const ShadePt& s
   return true;
 }
 
+// ---- 8-wide compressed traversal ----------------------------------------------
+
+// Byte k of w as a float: assemble 2^23 + byte in one byte permute, subtract
+// 2^23 (exact).
+__device__ __forceinline__ float qbyte(uint32_t w, int k) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | (unsigned)k)) - 8388608.0f;
+}
+
+__device__ __forceinline__ float expScale(uint32_t ew, int axis) {
+  int e = (int)(signed char)((ew >> (8 * axis)) & 0xFFu);
+  return __uint_as_float((uint32_t)(e + 127) << 23);
+}
+
+// Tests the 8 child boxes of node `idx` against the ray (origin o, inverse
+// direction id, octant order rayOct, interval [tmin, tmax]). Returns the
+// node's child/primitive bases, the internal children hit (bit i ^ rayOct
+// for slot i, so the lowest set bit is the nearest-first candidate) and the
+// primitives of the leaf children hit (bits relative to primBase).
+struct CwHits {
+  uint32_t childBase, primBase, imask, hits, leafBits, valid;
+};
+__device__ __forceinline__ CwHits cwIntersect(const CwNode* nodes, int idx, float3 o, float3 id,
+                                              uint32_t rayOct, float tmin, float tmax) {
+  const float kFar = 1.00000024f;
+  const float4* p4 = reinterpret_cast<const float4*>(nodes + idx);
+  float4 a = __ldg(p4), b = __ldg(p4 + 1), c = __ldg(p4 + 2), d = __ldg(p4 + 3), e = __ldg(p4 + 4);
+  uint32_t ew = __float_as_uint(a.w);
+  CwHits r;
+  r.imask = ew >> 24;
+  r.childBase = __float_as_uint(b.x);
+  r.primBase = __float_as_uint(b.y);
+  uint32_t meta[2] = {__float_as_uint(b.z), __float_as_uint(b.w)};
+  float sx = expScale(ew, 0) * id.x, sy = expScale(ew, 1) * id.y, sz = expScale(ew, 2) * id.z;
+  float ox = (a.x - o.x) * id.x, oy = (a.y - o.y) * id.y, oz = (a.z - o.z) * id.z;
+  // Near / far planes per axis: lo words give the near plane unless the
+  // direction is negative on that axis.
+  uint32_t lx[2] = {__float_as_uint(c.x), __float_as_uint(c.y)};
+  uint32_t ly[2] = {__float_as_uint(c.z), __float_as_uint(c.w)};
+  uint32_t lz[2] = {__float_as_uint(d.x), __float_as_uint(d.y)};
+  uint32_t hx[2] = {__float_as_uint(d.z), __float_as_uint(d.w)};
+  uint32_t hy[2] = {__float_as_uint(e.x), __float_as_uint(e.y)};
+  uint32_t hz[2] = {__float_as_uint(e.z), __float_as_uint(e.w)};
+  uint32_t nx[2], ny[2], nz[2], fx[2], fy[2], fz[2];
+#pragma unroll
+  for (int w = 0; w < 2; w++) {
+    bool sxn = id.x < 0.0f, syn = id.y < 0.0f, szn = id.z < 0.0f;
+    nx[w] = sxn ? hx[w] : lx[w];
+    fx[w] = sxn ? lx[w] : hx[w];
+    ny[w] = syn ? hy[w] : ly[w];
+    fy[w] = syn ? ly[w] : hy[w];
+    nz[w] = szn ? hz[w] : lz[w];
+    fz[w] = szn ? lz[w] : hz[w];
+  }
+  r.hits = 0;
+  r.leafBits = 0;
+  r.valid = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    int w = i >> 2, k = i & 3;
+    uint32_t m = (meta[w] >> (8 * k)) & 0xFFu;
+    float tn = fmaxf(fmaxf(fmaf(qbyte(nx[w], k), sx, ox), fmaf(qbyte(ny[w], k), sy, oy)),
+                     fmaxf(fmaf(qbyte(nz[w], k), sz, oz), tmin));
+    float tf = fminf(fminf(fmaf(qbyte(fx[w], k), sx, ox), fmaf(qbyte(fy[w], k), sy, oy)),
+                     fminf(fmaf(qbyte(fz[w], k), sz, oz), tmax)) * kFar;
+    bool slot = m != 0u;
+    r.valid |= (slot ? 1u : 0u) << i;
+    bool hit = slot && tn <= tf;
+    bool inner = (r.imask >> i) & 1u;
+    if (hit && inner) r.hits |= 1u << (i ^ rayOct);
+    if (hit && !inner) r.leafBits |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+  }
+  return r;
+}
+
+struct RayCtx {
+  float3 o, d, id;
+  uint32_t rayOct;  // slot ^ rayOct orders children near to far
+  WtRay wt;
+};
+__device__ __forceinline__ void rayInit(RayCtx& r, float3 o, float3 d, bool tri) {
+  r.o = o;
+  r.d = d;
+  r.id = v3(safeInv(d.x), safeInv(d.y), safeInv(d.z));
+  uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+  r.rayOct = oct ^ 7u;
+  if (tri) r.wt = wtSetup(d);
+}
+
+constexpr int kCwStack = 48;
+constexpr uint32_t kGroupPrims = 1u << 31;   // entry holds a primitive group
+constexpr uint32_t kGroupMarker = 1u << 30;  // entry returns from a BLAS
+
+#ifndef SDB_TRAVERSE_INLINE
+#define SDB_TRAVERSE_INLINE __forceinline__
+#endif
+
+// The BVH format is a build-time choice of the kernels (SDB_WIDE_BVH): the
+// binary layout (BvhNode, 2 children per 64-byte node) or the compressed
+// 8-wide layout (CwNode). The host builds whichever bvhWidth() reports.
+#if SDB_WIDE_BVH
 // SHADOW = false: closest accepted hit, returns whether one was found.
 // SHADOW = true: returns false when occluded, else accumulates the
 // transparent-crossing terms into trProd / tau.
 template <bool SHADOW, bool COUNT = false>
-__device__ __forceinline__ bool traverse(const SdLaunch& lp, float3 O, float3 D, float tmax,
+__device__ SDB_TRAVERSE_INLINE bool traverse(const SdLaunch& lp, float3 O, float3 D, float tmax,
+                                             TraceHit& hit, float& trProd, float3& tau,
+                                             TraceCount* cnt = nullptr) {
+  if (lp.numInstances == 0) return SHADOW;
+  uint2 stack[kCwStack];
+  int sp = 0;
+  const float tmin = 0.0f;
+  const CwNode* nodes = lp.cw;
+  RayCtx ray;
+  rayInit(ray, O, D, false);
+  bool inBlas = false;
+  int curInst = -1;
+  bool found = false;
+  // Current node group: a virtual parent whose only child (slot 0) is the root.
+  uint32_t gBase = (uint32_t)lp.tlasRoot, gHits = 1u << (0u ^ ray.rayOct), gImask = 1u;
+  uint32_t tBase = 0, tBits = 0;
+
+  while (true) {
+    if (COUNT) countWarp(cnt, cnt->travIters, cnt->travLanes);
+    if (gHits) {
+      int b = __ffs(gHits) - 1;
+      gHits &= gHits - 1u;
+      uint32_t slot = (uint32_t)b ^ ray.rayOct;
+      int child = (int)(gBase + __popc(gImask & ((1u << slot) - 1u)));
+      if (gHits && sp < kCwStack) stack[sp++] = make_uint2(gBase, gHits | (gImask << 8));
+      CwHits h = cwIntersect(nodes, child, ray.o, ray.id, ray.rayOct, tmin, tmax);
+      if (COUNT) cnt->boxTests += __popc(h.valid);
+      gBase = h.childBase;
+      gHits = h.hits;
+      gImask = h.imask;
+      tBase = h.primBase;
+      tBits = h.leafBits;
+    }
+    while (tBits) {
+      int j = __ffs(tBits) - 1;
+      tBits &= tBits - 1u;
+      int prim = (int)tBase + j;
+      if (!inBlas) {
+        const SdInstance& in = lp.inst[prim];
+        float3 o2 = xfPoint(in.w2o, O), d2 = xfVec(in.w2o, D);
+        if (in.kind == GK_MESH) {
+          if (COUNT) cnt->blasEntries++;
+          // No room to suspend this level (deeper than any tree the builder
+          // makes): skip the instance rather than overflow.
+          if (sp + 3 > kCwStack) continue;
+          if (gHits) stack[sp++] = make_uint2(gBase, gHits | (gImask << 8));
+          if (tBits) stack[sp++] = make_uint2(tBase, tBits | kGroupPrims);
+          stack[sp++] = make_uint2(0xFFFFFFFFu, kGroupMarker);
+          inBlas = true;
+          curInst = prim;
+          rayInit(ray, o2, d2, true);
+          gBase = (uint32_t)lp.meshes[in.mesh].root;
+          gHits = 1u << (0u ^ ray.rayOct);
+          gImask = 1u;
+          tBits = 0;
+          break;
+        }
+        if (COUNT) cnt->quadTests++;
+        QHits qh = hitQuadric(in.kind, o2, d2, tmin, tmax);
+        for (int k = 0; k < qh.n; k++) {
+          const QHit& q = qh.h[k];
+          if (q.t >= tmax) continue;
+          bool front = dot(q.n, d2) < 0.0f;
+          if ((in.flags & kInstMasked) && !faceAccepts(lp, in, front, q.u, q.v)) continue;
+          if (SHADOW) {
+            if (!(in.flags & kInstTransmissive)) return false;
+            uint16_t mid = front ? (uint16_t)(in.mats & 0xFFFF) : (uint16_t)(in.mats >> 16);
+            ShadePt spt = quadShade(in, q.n, q.u, q.v, D);
+            if (!shadowCross(lp, spt, mid, q.t, D, trProd, tau)) return false;
+          } else {
+            tmax = q.t;
+            found = true;
+            hit.t = q.t;
+            hit.inst = prim;
+            hit.prim = 0;
+            hit.u = q.u;
+            hit.v = q.v;
+            hit.nq = q.n;
+            hit.front = front;
+          }
+        }
+        continue;
+      }
+      // Triangle of the current BLAS, in object space.
+      const float4* tp = lp.tris + 3 * (size_t)prim;
+      float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+      if (COUNT) cnt->triTests++;
+      float t, b1, b2;
+      float3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
+      if (!wtHit(ray.wt, ray.o, p0, p1, p2, tmin, tmax, t, b1, b2)) continue;
+      int tri = __float_as_int(a.w);
+      const SdInstance& in = lp.inst[curInst];
+      if (!(in.flags & (kInstMasked | kInstTransmissive))) {
+        if (SHADOW) return false;
+        tmax = t;
+        found = true;
+        hit.t = t;
+        hit.inst = curInst;
+        hit.prim = tri;
+        hit.u = b1;
+        hit.v = b2;
+        hit.front = dot(cross(p1 - p0, p2 - p0), ray.d) < 0.0f;
+        continue;
+      }
+      ShadePt spt = triShade(lp, in, tri, b1, b2, D);
+      if ((in.flags & kInstMasked) && !faceAccepts(lp, in, spt.front, spt.u, spt.v)) continue;
+      if (SHADOW) {
+        if (!(in.flags & kInstTransmissive)) return false;
+        uint16_t mid = spt.front ? (uint16_t)(in.mats & 0xFFFF) : (uint16_t)(in.mats >> 16);
+        if (!shadowCross(lp, spt, mid, t, D, trProd, tau)) return false;
+      } else {
+        tmax = t;
+        found = true;
+        hit.t = t;
+        hit.inst = curInst;
+        hit.prim = tri;
+        hit.u = b1;
+        hit.v = b2;
+        hit.front = spt.front;
+      }
+    }
+    if (gHits || tBits) continue;
+    // Both groups exhausted: take the next entry.
+    bool done = true;
+    while (sp > 0) {
+      uint2 e = stack[--sp];
+      if (e.y & kGroupMarker) {
+        inBlas = false;
+        rayInit(ray, O, D, false);
+        continue;
+      }
+      if (e.y & kGroupPrims) {
+        tBase = e.x;
+        tBits = e.y & 0xFFFFFFu;
+      } else {
+        gBase = e.x;
+        gHits = e.y & 0xFFu;
+        gImask = (e.y >> 8) & 0xFFu;
+      }
+      done = false;
+      break;
+    }
+    if (done) break;
+  }
+  return SHADOW ? true : found;
+}
+
+#else
+// SHADOW = false: closest accepted hit, returns whether one was found.
+// SHADOW = true: returns false when occluded, else accumulates the
+// transparent-crossing terms into trProd / tau.
+template <bool SHADOW, bool COUNT = false>
+__device__ SDB_TRAVERSE_INLINE bool traverse(const SdLaunch& lp, float3 O, float3 D, float tmax,
                                          TraceHit& hit, float& trProd, float3& tau,
                                          TraceCount* cnt = nullptr) {
   if (lp.numInstances == 0) return SHADOW;
@@ -264,6 +532,7 @@ __device__ __forceinline__ bool traverse(const SdLaunch& lp, float3 O, float3 D,
   int cur = lp.tlasRoot;
 
   while (true) {
+    if (COUNT) countWarp(cnt, cnt->travIters, cnt->travLanes);
     if (cur >= 0) {
       BvhNode nd = loadNode(nodes, cur);
       if (COUNT) cnt->boxTests += 2;
@@ -394,4 +663,6 @@ __device__ __forceinline__ bool traverse(const SdLaunch& lp, float3 O, float3 D,
   return SHADOW ? true : found;
 }
 
+
+#endif
 }  // namespace sdb

@@ -107,7 +107,7 @@ struct SdMesh {
   const float3* pos;
   const float3* nrm;   // null: geometric normal
   const float2* uv;    // null: barycentric uv
-  int root;            // first node of this mesh's BLAS in SdLaunch::nodes
+  int root;            // this mesh's BLAS root in SdLaunch::cw
   int numTris;
 };
 
@@ -120,6 +120,23 @@ struct __align__(16) BvhNode {
   float4 zz;    // c0 lo.z hi.z, c1 lo.z hi.z
   int4 link;    // child0, child1, cnt0, cnt1
 };
+
+// Compressed 8-wide node (80 bytes, five 16-byte loads), after Ylitie,
+// Karras and Laine, "Efficient Incoherent Ray Traversal on GPUs Through
+// Compressed Wide BVHs" (HPG 2017). Child boxes are stored as 8-bit offsets
+// on a per-node grid: child lo = p + qlo * 2^e, hi = p + qhi * 2^e, rounded
+// outward when built so no hit is lost. Internal children are stored
+// contiguously from childBase; leaf primitives contiguously from primBase.
+// Slots are assigned so that visiting them in increasing slot ^ (ray octant
+// ^ 7) order is approximately front to back.
+//   a: p.x p.y p.z | e.x e.y e.z (int8) imask (bit s: slot s is internal)
+//   b: childBase | primBase | meta[0..3] | meta[4..7]
+//      meta (leaf slots): count << 5 | offset from primBase; 0 = empty slot
+//   c: qlo.x[8] qlo.y[8]   d: qlo.z[8] qhi.x[8]   e: qhi.y[8] qhi.z[8]
+struct __align__(16) CwNode {
+  float4 a, b, c, d, e;
+};
+constexpr int kCwLeafMax = 3;  // primitives per leaf slot
 
 // Everything a launch needs, in constant memory.
 struct SdLaunch {
@@ -161,6 +178,7 @@ struct SdLaunch {
   int numFlames;
 
   const BvhNode* nodes;
+  const CwNode* cw;       // 8-wide nodes (TLAS root first, then each BLAS)
   const float4* tris;     // 3 float4 per leaf-ordered triangle; .w of the
                           // first holds the mesh-local triangle index
   const SdInstance* inst;

@@ -10,6 +10,17 @@
 #include "sd_rng.cuh"
 #include "sd_types.h"
 
+// Paths most pixels never take (water normals, flame marches, quadric
+// roots) are compiled out of line in device code, keeping the hot loop's
+// instruction footprint small; host code inlines them as usual.
+#ifndef SDB_COLD
+#if defined(__CUDA_ARCH__)
+#define SDB_COLD static __host__ __device__ __noinline__
+#else
+#define SDB_COLD static inline
+#endif
+#endif
+
 namespace sdb {
 
 // Smoothstep that also accepts inverted edges. (device/noise.cuh:12-15)
@@ -67,7 +78,7 @@ SDB_HD float fbm3(float3 p, unsigned seed) {
 // Wave normal from an fBm height field over world xz by central differences;
 // falls back to ns when the perturbed normal would face away from wo.
 // (device/noise.cuh:67-79)
-SDB_HD float3 waveNormal(float3 x, float3 ns, float3 wo, float amp, float freq) {
+SDB_COLD float3 waveNormal(float3 x, float3 ns, float3 wo, float amp, float freq) {
   const unsigned seed = 1337u;
   const float e = 0.05f;
   float3 p = v3(x.x * freq, 0.0f, x.z * freq);
@@ -137,7 +148,7 @@ SDB_HD bool flameClip(const SdFlame& fl, float3 o, float3 d, float& t0, float& t
 // Emission along [1e-4, tEnd] of o + t d through every flame, weighted by the
 // running transmittance; the segment's transmittance is folded into trans.
 // One draw per entered flame. (device/volume.cuh:90-115)
-SDB_HD float3 flameMarch(const SdFlame* fls, int nfl, float3 o, float3 d, float tEnd,
+SDB_COLD float3 flameMarch(const SdFlame* fls, int nfl, float3 o, float3 d, float tEnd,
                          Pcg& rng, float3& trans) {
   float3 Lv = v3(0.0f);
   for (int i = 0; i < nfl; i++) {
@@ -167,7 +178,7 @@ SDB_HD float3 flameMarch(const SdFlame* fls, int nfl, float3 o, float3 d, float 
 // Transmittance-only twin of flameMarch for shadow segments: same steps, same
 // jitter draw, same exponentials; skip exempts a light's owning flame.
 // (device/volume.cuh:129-153)
-SDB_HD float flameShadow(const SdFlame* fls, int nfl, float3 o, float3 d, float tEnd,
+SDB_COLD float flameShadow(const SdFlame* fls, int nfl, float3 o, float3 d, float tEnd,
                          Pcg& rng, int skip) {
   float tr = 1.0f;
   for (int i = 0; i < nfl; i++) {

@@ -8,6 +8,7 @@
 
 #include "../../include/sundog_api.h"
 #include "abi_util.h"
+#include "bvh_build.h"
 #include "render_session.h"
 #include "sd_bsdf.cuh"
 #include "sd_lights.cuh"
@@ -236,6 +237,76 @@ extern "C" int sundog_selftest(int which, const void* in, int n, void* out, size
   cudaCheck(cudaGetLastError(), "selftest launch");
   cudaCheck(cudaDeviceSynchronize(), "selftest");
   cudaCheck(cudaMemcpy(out, dout.ptr, ob * n, cudaMemcpyDeviceToHost), "selftest download");
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+// Host-side structural check of the 8-wide BVH builder over caller boxes
+// (n boxes as lo.xyz, hi.xyz floats): every primitive is referenced by
+// exactly one leaf slot, every decoded (quantised) child box contains the
+// exact bounds of its subtree, leaf slots hold 1..3 primitives, internal
+// children are contiguous. out (6 u64): nodes, max depth, leaf slots,
+// internal slots, total slots tested per full sweep, failures.
+extern "C" __attribute__((visibility("default"))) int sundog_bvh_validate(const float* boxes, int n,
+                                                                          int leafMax,
+                                                                          unsigned long long* out) {
+  SDB_TRY
+  std::vector<Box3> bx((size_t)n);
+  for (int i = 0; i < n; i++) {
+    bx[i].lo = v3(boxes[6 * i], boxes[6 * i + 1], boxes[6 * i + 2]);
+    bx[i].hi = v3(boxes[6 * i + 3], boxes[6 * i + 4], boxes[6 * i + 5]);
+  }
+  CwBuild b = buildCw(bx, leafMax, 0, 0);
+  std::vector<int> seen((size_t)n, 0);
+  unsigned long long leaves = 0, inner = 0, fails = 0;
+  // subtree bounds by recursion from the root
+  struct Rec {
+    static Box3 walk(const CwBuild& b, const std::vector<Box3>& bx, int idx, std::vector<int>& seen,
+                     unsigned long long& leaves, unsigned long long& inner, unsigned long long& fails) {
+      const CwNode& nd = b.nodes[idx];
+      uint32_t w[4];
+      std::memcpy(w, &nd.a, 16);
+      uint32_t imask = w[3] >> 24;
+      uint32_t bw[4];
+      std::memcpy(bw, &nd.b, 16);
+      Box3 all = boxEmpty();
+      int innerSeen = 0;
+      for (int s = 0; s < 8; s++) {
+        uint32_t m = (bw[2 + (s >> 2)] >> (8 * (s & 3))) & 0xFFu;
+        if (!m) continue;
+        Box3 q = cwChildBox(nd, s);
+        Box3 exact = boxEmpty();
+        if (imask & (1u << s)) {
+          inner++;
+          exact = walk(b, bx, (int)bw[0] + innerSeen, seen, leaves, inner, fails);
+          innerSeen++;
+        } else {
+          leaves++;
+          int cntp = (int)(m >> 5), off = (int)(m & 31);
+          if (cntp < 1 || cntp > kCwLeafMax) fails++;
+          for (int k = 0; k < cntp; k++) {
+            int prim = b.order[bw[1] + off + k];
+            seen[prim]++;
+            boxGrow(exact, bx[prim]);
+          }
+        }
+        if (q.lo.x > exact.lo.x || q.lo.y > exact.lo.y || q.lo.z > exact.lo.z ||
+            q.hi.x < exact.hi.x || q.hi.y < exact.hi.y || q.hi.z < exact.hi.z)
+          fails++;
+        boxGrow(all, exact);
+      }
+      return all;
+    }
+  };
+  if (n > 0) Rec::walk(b, bx, 0, seen, leaves, inner, fails);
+  for (int i = 0; i < n; i++)
+    if (seen[i] != 1) fails++;
+  out[0] = b.nodes.size();
+  out[1] = (unsigned long long)b.maxDepth;
+  out[2] = leaves;
+  out[3] = inner;
+  out[4] = leaves + inner;
+  out[5] = fails;
   return SUNDOG_OK;
   SDB_CATCH(SUNDOG_ERROR)
 }
