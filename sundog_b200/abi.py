@@ -104,6 +104,7 @@ ADDITIVE_SYMBOLS = [
     "sundog_selftest", "sundog_session_create", "sundog_session_render",
     "sundog_session_read", "sundog_session_info", "sundog_session_destroy",
     "sundog_session_trace_counts", "sundog_transfer_bytes",
+    "sundog_session_render_tile_noalloc",
 ]
 
 _lib = None
@@ -167,6 +168,8 @@ def load(path=None):
     lib.sundog_session_trace_counts.argtypes = [vp, ctypes.POINTER(TraceCounts)]
     lib.sundog_transfer_bytes.argtypes = [ctypes.POINTER(ctypes.c_uint64)] * 2
     lib.sundog_transfer_bytes.restype = None
+    lib.sundog_session_render_tile_noalloc.argtypes = [vp, ip, ip, ip, ip, ip, ip, vp,
+                                                       ctypes.POINTER(ctypes.c_uint64), vp]
     lib.sundog_session_destroy.argtypes = [vp]
     lib.sundog_session_destroy.restype = None
     if path is None:

@@ -1,0 +1,267 @@
+// Per-path device code shared by the path kernels: camera sample, one path
+// segment (trace, media, surface or escape, NEE, BSDF sample, roulette),
+// AOV and radiance bookkeeping. Restates device/programs.cu:311-572 (cited
+// inline).
+#pragma once
+
+#include "kernels.h"
+#include "sd_bsdf.cuh"
+#include "sd_guide.cuh"
+#include "sd_lights.cuh"
+#include "sd_trace.cuh"
+#include "sd_volume.cuh"
+
+namespace sdb {
+
+__device__ __forceinline__ float3 sanitize3(float3 c) {
+  if (!isfinite(c.x) || !isfinite(c.y) || !isfinite(c.z)) return v3(0.0f);
+  return c;
+}
+
+__device__ __forceinline__ float3 background(const SdLaunch& lp, float3 dir) {
+  if (lp.bgKind == BG_ENVMAP) return envRadiance(lp.env, dir);
+  if (lp.bgKind == BG_GRADIENT) {
+    float t = 0.5f * (dir.y + 1.0f);
+    return lp.bgA + (lp.bgB - lp.bgA) * t;
+  }
+  return lp.bgA;
+}
+
+// Straight-line transmittance toward a light (device/programs.cu:70-85).
+template <bool COUNT>
+__device__ __forceinline__ float3 shadowTransmittance(const SdLaunch& lp, float3 o, float3 d,
+                                                      float tmax, TraceCount* cnt) {
+  TraceHit dummy;
+  float trProd = 1.0f;
+  float3 tau = v3(0.0f);
+  if (!traverse<true, COUNT>(lp, o, d, tmax, dummy, trProd, tau, cnt)) return v3(0.0f);
+  tau = v3(fmaxf(0.0f, tau.x), fmaxf(0.0f, tau.y), fmaxf(0.0f, tau.z));
+  float3 tr = v3(trProd);
+  if (hmax(tau) > 0.0f) tr = tr * vexp(-tau);
+  return tr;
+}
+
+struct Path {
+  float3 o, d, beta, L, prevX;
+  float prevPdf;
+  Pcg rng;
+  unsigned long long med;  // medium stack: 4 x 16-bit material ids
+  int medDepth;
+  int depth;
+  int pixel;
+  int s;
+  int slot;
+  bool specular;
+};
+
+__device__ __forceinline__ uint16_t medAt(unsigned long long med, int i) {
+  return (uint16_t)((med >> (16 * i)) & 0xFFFFull);
+}
+
+// Camera sample for path index id; false if the index is tile padding.
+// (device/programs.cu:312-357)
+__device__ __forceinline__ bool startPath(const SdLaunch& lp, unsigned long long id, Path& p) {
+  int sLocal = (int)(id / (unsigned long long)lp.npixPad);
+  int rem = (int)(id - (unsigned long long)sLocal * lp.npixPad);
+  int tile = rem >> 6, within = rem & 63;
+  int tx = tile % lp.tilesX, ty = tile / lp.tilesX;
+  int px = tx * 8 + (within & 7), py = ty * 8 + (within >> 3);
+  if (px >= lp.width || py >= lp.height) return false;
+  int pixel = py * lp.width + px;
+  int s = lp.sampleOffset + sLocal;
+  p.pixel = pixel;
+  p.s = s;
+  p.slot = sLocal * (lp.width * lp.height) + pixel;
+  p.rng = Pcg::seeded(((unsigned long long)pixel << 32) ^ (unsigned long long)s,
+                      (unsigned long long)lp.seed);
+  int ns = lp.nStrata;
+  float jx, jy;
+  if (s < ns * ns) {
+    jx = ((s % ns) + p.rng.uni()) / ns;
+    jy = ((s / ns) + p.rng.uni()) / ns;
+  } else {
+    jx = p.rng.uni();
+    jy = p.rng.uni();
+  }
+  float u = (px + jx) / lp.width;
+  float v = ((lp.height - 1 - py) + jy) / lp.height;
+  const SdCamera& cam = lp.cam;
+  float3 org = cam.origin;
+  if (cam.lensRadius > 0.0f) {
+    float2 rd = diskConcentric(p.rng.uni2());
+    rd.x *= cam.lensRadius;
+    rd.y *= cam.lensRadius;
+    org = org + cam.u * rd.x + cam.v * rd.y;
+  }
+  p.d = unit(cam.lowerLeft + u * cam.horizontal + v * cam.vertical - org);
+  p.o = org;
+  p.prevX = org;
+  p.L = v3(0.0f);
+  p.beta = v3(1.0f);
+  p.prevPdf = 0.0f;
+  p.specular = true;
+  p.med = 0ull;
+  p.medDepth = 0;
+  p.depth = 0;
+  return true;
+}
+
+__device__ __forceinline__ void addClamped(const SdLaunch& lp, Path& p, float3 c) {
+  if (p.depth >= 1 && lp.clampVal > 0.0f) c = vmin(c, v3(lp.clampVal));
+  p.L += c;
+}
+
+__device__ __forceinline__ void writeAov(const SdLaunch& lp, const Path& p, float3 alb, float3 nrm) {
+  if (!lp.aovOn) return;
+  lp.sampleAlb[p.slot] = make_float4(alb.x, alb.y, alb.z, 1.0f);
+  lp.sampleNrm[p.slot] = make_float4(nrm.x, nrm.y, nrm.z, 1.0f);
+}
+
+// One segment of the path: trace, media, surface or escape, NEE, BSDF
+// sample, roulette. Returns false when the path has ended.
+// (device/programs.cu:374-558)
+template <bool COUNT>
+__device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned long long& rays,
+                                       TraceCount* cnt) {
+  const bool hasEnv = lp.bgKind == BG_ENVMAP;
+  const int nStrat = lp.numLights + (hasEnv ? 1 : 0);
+
+  TraceHit h;
+  float dummyTr = 1.0f;
+  float3 dummyTau = v3(0.0f);
+  bool hit = traverse<false, COUNT>(lp, p.o, p.d, 1e16f, h, dummyTr, dummyTau, cnt);
+  rays++;
+
+  if (p.medDepth > 0) {
+    int top = min(p.medDepth, 4) - 1;
+    float3 sigma = lp.materials[medAt(p.med, top)].absorb;
+    if (hmax(sigma) > 0.0f) p.beta *= vexp(-sigma * (hit ? h.t : 1e4f));
+  }
+
+  if (lp.numFlames > 0) {
+    float3 trans = v3(1.0f);
+    float3 Lv = flameMarch(lp.flames, lp.numFlames, p.o, p.d, hit ? h.t : 1e16f, p.rng, trans);
+    addClamped(lp, p, p.beta * Lv);
+    p.beta *= trans;
+  }
+
+  if (!hit) {
+    float3 bg = background(lp, p.d);
+    float w = 1.0f;
+    if (hasEnv && !p.specular) {
+      float pdfE = envDensity(lp.env, p.d) / nStrat;
+      w = p.prevPdf / (p.prevPdf + pdfE);
+    }
+    addClamped(lp, p, p.beta * bg * w);
+    if (p.depth == 0) writeAov(lp, p, v3(fminf(bg.x, 1.0f), fminf(bg.y, 1.0f), fminf(bg.z, 1.0f)), v3(0.0f));
+    return false;
+  }
+
+  const SdInstance& in = lp.inst[h.inst];
+  ShadePt sp = in.kind == GK_MESH ? triShade(lp, in, h.prim, h.u, h.v, p.d)
+                                  : quadShade(in, h.nq, h.u, h.v, p.d);
+  bool front = h.front;
+  int matId = front ? (int)(in.mats & 0xFFFF) : (int)(in.mats >> 16);
+  float3 ns = front ? sp.nFront : -sp.nFront;
+  float3 x = p.o + h.t * p.d;
+  const SdMaterial mat = lp.materials[matId];
+  float3 albedo = surfaceAlbedo(mat, lp.textures, sp.u, sp.v);
+  if (mat.kind == MT_WATER && mat.waveAmp > 0.0f)
+    ns = waveNormal(x, ns, -p.d, mat.waveAmp, mat.waveFreq);
+
+  if (p.depth == 0) {
+    const SdCamera& cam = lp.cam;
+    writeAov(lp, p, albedo, v3(dot(ns, cam.u), dot(ns, cam.v), dot(ns, cam.w)));
+  }
+
+  if (mat.kind == MT_EMISSIVE) {
+    if (front || mat.twoSided) {
+      float3 Le = albedo * mat.intensity;
+      float w = 1.0f;
+      if (!p.specular && in.lightId >= 0 && lp.numLights > 0) {
+        float pdfL = lightDensity(lp.lights[in.lightId], p.prevX, x, ns) / nStrat;
+        w = p.prevPdf / (p.prevPdf + pdfL);
+      }
+      addClamped(lp, p, p.beta * Le * w);
+    }
+    return false;
+  }
+
+  // Relative index at this interface from the medium stack.
+  float etaExt = 1.0f;
+  if (mat.kind == MT_DIELECTRIC || mat.kind == MT_WATER) {
+    int outer = min(front ? p.medDepth : p.medDepth - 1, 4);
+    if (outer > 0) etaExt = lp.materials[medAt(p.med, outer - 1)].ior;
+  }
+  float etaRel = front ? etaExt / mat.ior : mat.ior / etaExt;
+
+  // Next-event estimation with the balance heuristic.
+  if (nStrat > 0 && !isDeltaMaterial(mat)) {
+    int k = min((int)(p.rng.uni() * nStrat), nStrat - 1);
+    LightDraw ls = k < lp.numLights ? lightDraw(lp.lights[k], x, p.rng, lp.textures)
+                                    : envDraw(lp.env, p.rng);
+    float cosS = ls.ok ? dot(ls.wi, ns) : 0.0f;
+    bool transmitNee = cosS < 0.0f && mat.kind == MT_DIELECTRIC;
+    if (ls.ok && (cosS > 0.0f || transmitNee)) {
+      rays++;
+      float3 so = nudge(x, transmitNee ? -ns : ns);
+      float tmaxS = ls.dist * 0.999f;
+      float3 tr = shadowTransmittance<COUNT>(lp, so, ls.wi, tmaxS, cnt);
+      if (hmax(tr) > 0.0f) {
+        if (lp.numFlames > 0 && lp.transparentShadows) {
+          int skip = k < lp.numLights ? lp.lights[k].flameId : -1;
+          tr = tr * flameShadow(lp.flames, lp.numFlames, so, ls.wi, tmaxS, p.rng, skip);
+        }
+        float pdfLe = (ls.delta ? 1.0f : ls.pdf) / nStrat;
+        float3 f = bsdfValue(mat, albedo, -p.d, ls.wi, ns, etaRel);
+        float w = 1.0f;
+        if (!ls.delta) {
+          float pdfB = bsdfDensity(mat, -p.d, ls.wi, ns, etaRel);
+          if (lp.guiding) pdfB = guideMixPdf(lp, x, ns, ls.wi, pdfB, mat);
+          w = pdfLe / (pdfLe + pdfB);
+        }
+        float3 c = p.beta * f * fabsf(cosS) * ls.Li * w / pdfLe;
+        c = c * tr;
+        if (p.depth >= 1 && lp.clampVal > 0.0f) c = vmin(c, v3(lp.clampVal));
+        p.L += sanitize3(c);
+      }
+    }
+  }
+
+  BsdfDraw bs;
+  if (lp.guiding && guideEligible(mat))
+    bs = guidedDraw(lp, mat, albedo, p.d, ns, front, etaExt, etaRel, x, p.rng);
+  else
+    bs = bsdfDraw(mat, albedo, p.d, ns, front, etaExt, p.rng);
+  if (!bs.ok) return false;
+  if ((mat.kind == MT_WATER || mat.kind == MT_DIELECTRIC) && dot(bs.wi, ns) < 0.0f) {
+    if (front) {
+      if (p.medDepth < 4) {
+        unsigned long long sh = 16ull * p.medDepth;
+        p.med = (p.med & ~(0xFFFFull << sh)) | ((unsigned long long)matId << sh);
+      }
+      p.medDepth++;
+    } else if (p.medDepth > 0) {
+      p.medDepth--;
+    }
+  }
+  if (lp.guiding && lp.guideTrain) guideRecord(lp, p.pixel, x, ns, bs.wi, p.beta, p.L);
+  p.beta *= bs.weight;
+  p.specular = bs.delta;
+  p.prevPdf = bs.delta ? 0.0f : bs.pdf;
+  p.prevX = x;
+  float3 offN = dot(bs.wi, ns) >= 0.0f ? ns : -ns;
+  p.o = nudge(x, offN);
+  p.d = bs.wi;
+
+  if (p.depth >= 4) {
+    float q = clampf(hmax(p.beta), 0.05f, 0.95f);
+    if (p.rng.uni() >= q) return false;
+    p.beta *= 1.0f / q;
+  }
+  if (hmax(p.beta) <= 0.0f) return false;
+  p.depth++;
+  return p.depth < lp.maxDepth;
+}
+
+}  // namespace sdb
