@@ -292,4 +292,67 @@ SUNDOG_API int sundog_scene_debug_json(sundog_scene*, char* buf, size_t cap,
 SUNDOG_API int sundog_selftest(int which, const void* in, int n, void* out,
                                size_t out_bytes);
 
+/* ---- Learned path guiding (no counterpart in the reference) -------------
+ * A small network (48 inputs: frequency-encoded position + normal; 3 hidden
+ * layers of 64, ReLU; 8 von Mises-Fisher lobes out), trained on the GPU from
+ * the renderer's own radiance samples and mixed into BSDF sampling by MIS,
+ * so a guided render stays unbiased. A guided render traces its first
+ * train_spp samples in passes of pass_spp; after each pass the network takes
+ * steps_per_pass Adam steps and its mixture table is re-baked; the rest of
+ * the samples use the final guide. Every sample goes to the film. */
+typedef struct {
+  int32_t train_spp;      /* samples whose paths train the network (32) */
+  int32_t pass_spp;       /* samples per training pass (4) */
+  int32_t steps_per_pass; /* Adam steps after each pass (64) */
+  int32_t batch;          /* training records per step (16384) */
+  float learning_rate;    /* Adam step size (5e-3) */
+  float mix;              /* probability of drawing from the guide, [0, 1) (0.5) */
+  uint64_t seed;          /* network initialisation and batch draws (1) */
+  uint64_t record_cap;    /* training records kept per pass (4194304) */
+} sundog_guiding_config;
+
+typedef struct {
+  uint64_t records;       /* records the last pass produced (may exceed the cap) */
+  int32_t passes;         /* training passes so far */
+  int32_t train_steps;    /* Adam steps so far */
+  double train_ms;        /* CUDA-event time of training, summed */
+  double bake_ms;         /* CUDA-event time of the mixture-table bakes, summed */
+  double last_loss;       /* mean batch loss of the last pass */
+  float box_lo[3], box_hi[3]; /* region the guide's grid covers */
+} sundog_guiding_stats;
+
+/* Fills *config with the defaults above. */
+SUNDOG_API void sundog_guiding_defaults(sundog_guiding_config* config);
+/* Turns guiding on (config NULL = defaults; the network starts untrained) or
+ * off (enable 0) for the session's later renders. A render with reset != 0
+ * retrains from scratch. sundog_render_ext.guiding = 1 at session creation
+ * (or in sundog_render_ex) is the same as enabling it with the defaults.
+ * Returns 0/1. */
+SUNDOG_API int sundog_session_set_guiding(sundog_session*, int enable,
+                                          const sundog_guiding_config* config);
+SUNDOG_API int sundog_session_guiding_stats(sundog_session*, sundog_guiding_stats*);
+/* The session's current network parameters (14576 floats, layout below). */
+SUNDOG_API int sundog_session_guide_params(sundog_session*, float* params);
+/* Training records of the last training pass (12 floats each: x, F/p, n, 0,
+ * wi, 0): *count receives how many the pass kept; at most max_records are
+ * copied to out (may be NULL). */
+SUNDOG_API int sundog_session_guide_records(sundog_session*, float* out, uint64_t max_records,
+                                            uint64_t* count);
+
+/* The network's kernels on caller-given parameters, for parity checks
+ * against a CPU restatement. params: 14576 floats (weight matrices row-major
+ * [out][in]: W0 64x48, W1 64x64, W2 64x64, W3 48x64; then biases 64, 64, 64,
+ * 48), rounded to BF16 for the weights. */
+/* Initial parameters for a seed. */
+SUNDOG_API int sundog_guide_init_params(uint64_t seed, float* params);
+/* Raw network outputs (n x 40) for queries (n x 6: position in [0,1]^3,
+ * normal). */
+SUNDOG_API int sundog_guide_outputs(const float* params, const float* queries, int n,
+                                    float* outputs);
+/* Loss and its gradient (14576 floats, parameter layout) over n training
+ * records (n x 12 floats: x, F/p, n, 0, wi, 0), all in one batch; box: guide
+ * box origin (3) and 1/extent (3). */
+SUNDOG_API int sundog_guide_gradients(const float* params, const float* records, int n,
+                                      const float* box, float* grads, float* loss);
+
 #endif /* SUNDOG_B200_API_H */

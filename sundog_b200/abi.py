@@ -84,6 +84,23 @@ class TraceCounts(ctypes.Structure):
                 ("loop_lanes", ctypes.c_uint64)]
 
 
+class GuidingConfig(ctypes.Structure):
+    _fields_ = [("train_spp", ctypes.c_int32), ("pass_spp", ctypes.c_int32),
+                ("steps_per_pass", ctypes.c_int32), ("batch", ctypes.c_int32),
+                ("learning_rate", ctypes.c_float), ("mix", ctypes.c_float),
+                ("seed", ctypes.c_uint64), ("record_cap", ctypes.c_uint64)]
+
+
+class GuidingStats(ctypes.Structure):
+    _fields_ = [("records", ctypes.c_uint64), ("passes", ctypes.c_int32),
+                ("train_steps", ctypes.c_int32), ("train_ms", ctypes.c_double),
+                ("bake_ms", ctypes.c_double), ("last_loss", ctypes.c_double),
+                ("box_lo", ctypes.c_float * 3), ("box_hi", ctypes.c_float * 3)]
+
+
+# Parameter count of the guiding network (include/sundog_api.h).
+GUIDE_PARAMS = 14576
+
 # Every symbol include/sundog_api.h declares (the first 27 are the drop-in
 # surface of the reference ABI).
 DROP_IN_SYMBOLS = [
@@ -104,7 +121,10 @@ ADDITIVE_SYMBOLS = [
     "sundog_selftest", "sundog_session_create", "sundog_session_render",
     "sundog_session_read", "sundog_session_info", "sundog_session_destroy",
     "sundog_session_trace_counts", "sundog_transfer_bytes",
-    "sundog_session_render_tile_noalloc",
+    "sundog_session_render_tile_noalloc", "sundog_guiding_defaults",
+    "sundog_session_set_guiding", "sundog_session_guiding_stats", "sundog_guide_init_params",
+    "sundog_guide_outputs", "sundog_guide_gradients", "sundog_session_guide_params",
+    "sundog_session_guide_records",
 ]
 
 _lib = None
@@ -172,6 +192,16 @@ def load(path=None):
                                                        ctypes.POINTER(ctypes.c_uint64), vp]
     lib.sundog_session_destroy.argtypes = [vp]
     lib.sundog_session_destroy.restype = None
+    lib.sundog_guiding_defaults.argtypes = [ctypes.POINTER(GuidingConfig)]
+    lib.sundog_guiding_defaults.restype = None
+    lib.sundog_session_set_guiding.argtypes = [vp, ip, ctypes.POINTER(GuidingConfig)]
+    lib.sundog_session_guiding_stats.argtypes = [vp, ctypes.POINTER(GuidingStats)]
+    lib.sundog_guide_init_params.argtypes = [ctypes.c_uint64, vp]
+    lib.sundog_guide_outputs.argtypes = [vp, vp, ip, vp]
+    lib.sundog_guide_gradients.argtypes = [vp, vp, ip, vp, vp, vp]
+    lib.sundog_session_guide_params.argtypes = [vp, vp]
+    lib.sundog_session_guide_records.argtypes = [vp, vp, ctypes.c_uint64,
+                                                 ctypes.POINTER(ctypes.c_uint64)]
     if path is None:
         _lib = lib
     return lib

@@ -23,7 +23,8 @@ cudaError_t setLaunch(const SdLaunch& lp, cudaStream_t st);
 // BVH layout the kernels were compiled for: 2 (BvhNode) or 8 (CwNode).
 int bvhWidth();
 int renderGridSize();
-cudaError_t launchRender(cudaStream_t st, int grid);
+// guide: 0 plain; kGuideSample / kGuideRecord bits select the guided variants.
+cudaError_t launchRender(cudaStream_t st, int grid, int guide = 0);
 cudaError_t launchFold(int npix, cudaStream_t st);
 struct TraceCount;  // sd_trace.cuh: four u64 counters
 // Same kernel with traversal visit counters (node box tests, triangle and

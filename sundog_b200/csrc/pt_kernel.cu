@@ -12,6 +12,10 @@
 // 560-563), which keeps the film bit-identical to a one-thread-per-pixel
 // sequential loop regardless of which thread traced which sample.
 //
+// Guided variants (GUIDE != 0, sd_guide.cuh) draw directions by MIS with the
+// learned guide and/or record training samples; GUIDE = 0 is the plain
+// reference sampler with no guiding code compiled in.
+//
 // The bounce body restates device/programs.cu:311-572 (cited inline).
 #include "pt_path.cuh"
 
@@ -19,7 +23,7 @@ namespace sdb {
 
 __constant__ SdLaunch c_lp;
 
-template <bool COUNT>
+template <bool COUNT, int GUIDE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_MIN_BLOCKS) ptPersistent(TraceCount* counts) {
   const SdLaunch& lp = c_lp;
   TraceCount cnt = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -31,6 +35,8 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_MIN_BLOCKS) ptPersistent(Tra
   bool exhausted = false;  // warp-uniform
   Path p;
   p.slot = 0;
+  GuideTrail trail;
+  trail.n = 0;
 
   while (true) {
     if (!exhausted) {
@@ -46,6 +52,7 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_MIN_BLOCKS) ptPersistent(Tra
           // Tile padding and indices past the end simply draw again next
           // round (padding) or leave the lane idle (past the end).
           if (id < lp.numPaths) active = startPath(lp, id, p);
+          if (GUIDE & kGuideRecord) trail.n = 0;
         }
       }
     }
@@ -55,8 +62,9 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_MIN_BLOCKS) ptPersistent(Tra
     }
     if (active) {
       if (COUNT) countWarp(&cnt, cnt.loopIters, cnt.loopLanes);
-      if (!bounce<COUNT>(lp, p, rays, &cnt)) {
+      if (!bounce<COUNT, GUIDE>(lp, p, rays, &cnt, &trail)) {
         float3 L = sanitize3(p.L);
+        if (GUIDE & kGuideRecord) guideFlush(lp, trail, L);
         lp.sampleL[p.slot] = make_float4(L.x, L.y, L.z, 1.0f);
         active = false;
       }
@@ -116,18 +124,26 @@ int renderGridSize() {
   int dev = 0, sms = 0, perSm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, ptPersistent<false>, kRenderBlock, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, ptPersistent<false, 0>, kRenderBlock, 0);
   if (perSm < 1) perSm = 1;
   return sms * perSm;
 }
 
-cudaError_t launchRender(cudaStream_t st, int grid) {
-  ptPersistent<false><<<grid, kRenderBlock, 0, st>>>(nullptr);
+cudaError_t launchRender(cudaStream_t st, int grid, int guide) {
+  switch (guide) {
+    case 0: ptPersistent<false, 0><<<grid, kRenderBlock, 0, st>>>(nullptr); break;
+    case kGuideSample: ptPersistent<false, kGuideSample><<<grid, kRenderBlock, 0, st>>>(nullptr); break;
+    case kGuideRecord: ptPersistent<false, kGuideRecord><<<grid, kRenderBlock, 0, st>>>(nullptr); break;
+    case kGuideSample | kGuideRecord:
+      ptPersistent<false, kGuideSample | kGuideRecord><<<grid, kRenderBlock, 0, st>>>(nullptr);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launchRenderCounting(cudaStream_t st, int grid, TraceCount* counts) {
-  ptPersistent<true><<<grid, kRenderBlock, 0, st>>>(counts);
+  ptPersistent<true, 0><<<grid, kRenderBlock, 0, st>>>(counts);
   return cudaGetLastError();
 }
 

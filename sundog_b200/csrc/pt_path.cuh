@@ -118,11 +118,13 @@ __device__ __forceinline__ void writeAov(const SdLaunch& lp, const Path& p, floa
 }
 
 // One segment of the path: trace, media, surface or escape, NEE, BSDF
-// sample, roulette. Returns false when the path has ended.
+// sample, roulette. Returns false when the path has ended. GUIDE selects the
+// guided variants (kGuideSample: draw by MIS with the guide; kGuideRecord:
+// keep training vertices in *trail); 0 is the reference's sampler.
 // (device/programs.cu:374-558)
-template <bool COUNT>
+template <bool COUNT, int GUIDE = 0>
 __device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned long long& rays,
-                                       TraceCount* cnt) {
+                                       TraceCount* cnt, GuideTrail* trail = nullptr) {
   const bool hasEnv = lp.bgKind == BG_ENVMAP;
   const int nStrat = lp.numLights + (hasEnv ? 1 : 0);
 
@@ -217,7 +219,6 @@ __device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned lon
         float w = 1.0f;
         if (!ls.delta) {
           float pdfB = bsdfDensity(mat, -p.d, ls.wi, ns, etaRel);
-          if (lp.guiding) pdfB = guideMixPdf(lp, x, ns, ls.wi, pdfB, mat);
           w = pdfLe / (pdfLe + pdfB);
         }
         float3 c = p.beta * f * fabsf(cosS) * ls.Li * w / pdfLe;
@@ -229,10 +230,15 @@ __device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned lon
   }
 
   BsdfDraw bs;
-  if (lp.guiding && guideEligible(mat))
-    bs = guidedDraw(lp, mat, albedo, p.d, ns, front, etaExt, etaRel, x, p.rng);
-  else
+  float pdfSample;  // density wi was drawn with (differs from bs.pdf when guided)
+  if ((GUIDE & kGuideSample) && guideEligible(mat)) {
+    GuidedDraw gd = guidedDraw(lp, mat, albedo, p.d, ns, front, etaExt, etaRel, x, p.rng);
+    bs = gd.s;
+    pdfSample = gd.pdfSample;
+  } else {
     bs = bsdfDraw(mat, albedo, p.d, ns, front, etaExt, p.rng);
+    pdfSample = bs.pdf;
+  }
   if (!bs.ok) return false;
   if ((mat.kind == MT_WATER || mat.kind == MT_DIELECTRIC) && dot(bs.wi, ns) < 0.0f) {
     if (front) {
@@ -245,7 +251,8 @@ __device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned lon
       p.medDepth--;
     }
   }
-  if (lp.guiding && lp.guideTrain) guideRecord(lp, p.pixel, x, ns, bs.wi, p.beta, p.L);
+  if ((GUIDE & kGuideRecord) && !bs.delta && guideEligible(mat))
+    guideRecord(*trail, x, ns, bs.wi, pdfSample, p.beta * bs.weight, p.L);
   p.beta *= bs.weight;
   p.specular = bs.delta;
   p.prevPdf = bs.delta ? 0.0f : bs.pdf;

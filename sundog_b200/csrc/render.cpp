@@ -22,6 +22,7 @@
 #include "abi_util.h"
 #include "assets.h"
 #include "bvh_build.h"
+#include "guide.h"
 #include "kernels.h"
 #include "render_session.h"
 #include "scene_model.h"
@@ -471,14 +472,26 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
   l.tlasRoot = 0;
   l.numInstances = nObj;
   grid = renderGridSize();
+  if (ext && ext->guiding) setGuiding(true, nullptr);
   cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
   deviceBytes = freeBefore > freeB ? freeBefore - freeB : 0;
   setupMs = msSince(tTotal);
 }
 
+void RenderSession::setGuiding(bool enable, const sundog_guiding_config* cfg) {
+  if (!enable) {
+    guide.reset();
+    return;
+  }
+  std::unique_ptr<GuideState> g(new GuideState());
+  g->configure(cfg ? *cfg : guideDefaults());
+  guide = std::move(g);
+}
+
 void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* res) {
   if (!st) st = stream;
   size_t npix = (size_t)lp.width * lp.height;
+  if (guide && reset) guide->reset();
   if (reset) {
     cudaCheck(cudaMemsetAsync(accum.ptr, 0, accum.bytes, st), "film reset");
     if (aov) {
@@ -495,13 +508,18 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
   float kms = 0.0f;
   while (done < lp.sppTotal) {
     int n = std::min(chunk, lp.sppTotal - done);
+    int mode = guide ? guide->kernelMode() : 0;
+    if (mode & kGuideRecord) {
+      n = std::min(n, std::min(guide->cfg.pass_spp, guide->cfg.train_spp - guide->trainedSpp));
+      guide->beginPass(lp, st);
+    }
     lp.sampleOffset = sampleBase + done;
     lp.sppThisLaunch = n;
     lp.numPaths = (unsigned long long)lp.npixPad * n;
     cudaCheck(cudaMemsetAsync(lp.pathCounter, 0, sizeof(unsigned long long), st), "counter reset");
     cudaCheck(setLaunch(lp, st), "launch params");
     cudaCheck(cudaEventRecord(kev[0], st), "event");
-    cudaCheck(launchRender(st, grid), "path kernel launch");
+    cudaCheck(launchRender(st, grid, mode), "path kernel launch");
     cudaCheck(cudaEventRecord(kev[1], st), "event");
     cudaCheck(cudaEventSynchronize(kev[1]), "path kernel");
     float one = 0.0f;
@@ -510,6 +528,10 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
     cudaCheck(launchFold((int)npix, st), "fold launch");
     launches += 2;
     done += n;
+    if (mode & kGuideRecord) {
+      guide->trainAndBake(lp, st, n);
+      launches += 2 + 2 * guide->cfg.steps_per_pass;
+    }
   }
   cudaCheck(cudaEventRecord(ev1, st), "event");
   cudaCheck(cudaStreamSynchronize(st), "path kernels");
@@ -679,6 +701,29 @@ extern "C" int sundog_session_trace_counts(sundog_session* sh, sundog_trace_coun
   SDB_TRY
   if (!sh || !out) throw std::runtime_error("session: null argument");
   reinterpret_cast<RenderSession*>(sh)->countTraversal(out);
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" void sundog_guiding_defaults(sundog_guiding_config* c) {
+  if (c) *c = guideDefaults();
+}
+
+extern "C" int sundog_session_set_guiding(sundog_session* sh, int enable,
+                                          const sundog_guiding_config* cfg) {
+  SDB_TRY
+  if (!sh) throw std::runtime_error("session: null handle");
+  reinterpret_cast<RenderSession*>(sh)->setGuiding(enable != 0, cfg);
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_session_guiding_stats(sundog_session* sh, sundog_guiding_stats* out) {
+  SDB_TRY
+  if (!sh || !out) throw std::runtime_error("session: null argument");
+  const RenderSession* s = reinterpret_cast<RenderSession*>(sh);
+  if (!s->guide) throw std::runtime_error("session: guiding is not enabled");
+  *out = s->guide->stats;
   return SUNDOG_OK;
   SDB_CATCH(SUNDOG_ERROR)
 }

@@ -17,6 +17,7 @@
 
 #include "../../include/sundog_api.h"
 #include "abi_util.h"
+#include "guide.h"
 #include "render_session.h"
 
 using namespace sdb;

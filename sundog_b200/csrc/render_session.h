@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -39,6 +40,8 @@ void buildMeshLightCdf(const std::vector<float3>& wp, const std::vector<uint3>& 
                        std::vector<float>& cdf, double& total);
 void quadricBoundsHost(int kind, float3& lo, float3& hi);
 
+struct GuideState;  // guide.h
+
 struct RenderSession {
   SceneDesc scene;
   SdLaunch lp{};
@@ -63,12 +66,14 @@ struct RenderSession {
   std::vector<DevBuf> lightBufs;
   DevBuf dNodes, dTris, dInst, dMeshes, dTex, dMat, dLights, dFlames;
   DevBuf accum, aovAlb, aovNrm, sampleL, sampleAlb, sampleNrm, counters;
+  std::unique_ptr<GuideState> guide;  // learned path guiding, when enabled
 
   ~RenderSession();
   void build(const sundog_scene* h, const sundog_render_options* opt, const sundog_render_ext* ext);
   void render(cudaStream_t st, bool reset, sundog_render_result* res);
   void read(float* film, float* alb, float* nrm);
   void countTraversal(sundog_trace_counts* out);
+  void setGuiding(bool enable, const sundog_guiding_config* cfg);
 };
 
 }  // namespace sdb

@@ -186,11 +186,13 @@ struct SdLaunch {
   int tlasRoot;
   int numInstances;
 
-  // learned path guiding (optional)
-  int guiding;
-  const void* guideNet;
-  float guideMix;
-  float* guideTrain;
+  // learned path guiding (read only by the guided kernel variants)
+  const float4* guideLobes;   // [cells][8] lobes: kappa*mu, log pdf coefficient
+  const float* guideCdf;      // [cells][8] cumulative lobe weights
+  float3 guideLo;             // grid origin and 1 / extent
+  float3 guideInvExtent;
+  float guideMix;             // probability of drawing from the guide
+  float4* guideTrain;         // training records, 3 float4 each
   unsigned long long* guideTrainCount;
   unsigned long long guideTrainCap;
 };

@@ -343,6 +343,42 @@ class Session(object):
                                                  ctypes.byref(res)), "session render", self.lib)
         return res
 
+    def set_guiding(self, enable=True, **cfg):
+        """Learned path guiding for later renders; cfg overrides defaults
+        (train_spp, pass_spp, steps_per_pass, batch, learning_rate, mix, seed,
+        record_cap)."""
+        c = abi.GuidingConfig()
+        self.lib.sundog_guiding_defaults(ctypes.byref(c))
+        for k, v in cfg.items():
+            if not hasattr(c, k):
+                raise TypeError("unknown guiding option %r" % k)
+            setattr(c, k, v)
+        abi.check(self.lib.sundog_session_set_guiding(self.handle, 1 if enable else 0,
+                                                      ctypes.byref(c)), "guiding", self.lib)
+
+    def guiding_stats(self):
+        st = abi.GuidingStats()
+        abi.check(self.lib.sundog_session_guiding_stats(self.handle, ctypes.byref(st)),
+                  "guiding stats", self.lib)
+        return st
+
+    def guide_params(self):
+        p = np.zeros(abi.GUIDE_PARAMS, np.float32)
+        abi.check(self.lib.sundog_session_guide_params(self.handle, p.ctypes.data), "guide params",
+                  self.lib)
+        return p
+
+    def guide_records(self, max_records=1 << 20):
+        n = ctypes.c_uint64(0)
+        abi.check(self.lib.sundog_session_guide_records(self.handle, None, 0, ctypes.byref(n)),
+                  "guide records", self.lib)
+        m = min(n.value, max_records)
+        out = np.zeros((m, 12), np.float32)
+        abi.check(self.lib.sundog_session_guide_records(self.handle, out.ctypes.data, m,
+                                                        ctypes.byref(n)), "guide records",
+                  self.lib)
+        return out
+
     def read(self):
         s = self.stats
         film = np.zeros((s.height, s.width, 4), np.float32)
