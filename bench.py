@@ -64,6 +64,10 @@ def parse_args():
     ap.add_argument("--guide-spp", type=int, default=256)
     ap.add_argument("--guide-ref-spp", type=int, default=16384)
     ap.add_argument("--guide-seeds", type=int, default=4)
+    ap.add_argument("--serving", action="store_true",
+                    help="render-server line (Poisson jobs, p50/p99 latency) instead of Mrays/s")
+    ap.add_argument("--serve-jobs", type=int, default=60)
+    ap.add_argument("--serve-rate", type=float, default=20.0)
     return ap.parse_args()
 
 
@@ -448,12 +452,92 @@ def run_guiding(args):
     return 0
 
 
+# ---- serving: Poisson-arriving jobs, continuous batching ----------------------------------
+
+def run_serving(args):
+    """Render server under Poisson arrivals (rate 20/s, seed 5): each job
+    draws a scene from the Cornell / instancing / volumes configs, a square
+    resolution log-uniform in 256..2048 and spp log-uniform in 4..256, and is
+    submitted at its arrival time; the server batches 64x64 tile-passes of all
+    admitted jobs into each persistent launch. Reports p50 / p99 job latency
+    (submission -> film on the host) and aggregate Mrays/s over the run.
+    Prints one JSON line."""
+    from sundog_b200 import serve, workloads
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    ad = asset_dir()
+    scenes = [workloads.cornell(), workloads.instancing(ad), workloads.volumes(ad)]
+    rng = np.random.default_rng(5)
+    n = args.serve_jobs
+    gaps = rng.exponential(1.0 / args.serve_rate, n)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    kinds = rng.integers(0, 3, n)
+    sides = np.exp(rng.uniform(np.log(256), np.log(2048), n)).astype(int)
+    spps = np.exp(rng.uniform(np.log(4), np.log(256), n)).round().astype(int)
+    work = [(int(k), int(w), int(p)) for k, w, p in zip(kinds, sides, spps)]
+    # Warm-up: every scene once (module load, scene builds), then a fresh
+    # server for the timed run so no scene is resident when it starts.
+    with serve.Server() as sv:
+        for s in scenes:
+            sv.submit(s, base_dir=ad, width=64, height=64, spp=1, film=False).wait()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    with serve.Server() as sv:
+        t0 = time.perf_counter()
+        jobs = []
+        for (k, side, spp), at in zip(work, arrivals):
+            delay = t0 + at - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            jobs.append(sv.submit(scenes[k], base_dir=ad, width=side, height=side, spp=spp,
+                                  seed=1 + len(jobs)))
+        lat, queued, failed = [], [], 0
+        for j in jobs:
+            try:
+                j.wait()
+            except serve.JobError:
+                failed += 1
+            lat.append(j.last.latency_ms)
+            queued.append(j.last.queued_ms)
+            j.film = None
+        wall = time.perf_counter() - t0
+        st = sv.stats()
+    clocks = sampler.stop()
+    paths_total = sum(side * side * spp for _, side, spp in work)
+    line = {
+        "metric": "serving: aggregate Mrays/s; p50/p99 job latency", "value": st.rays / wall / 1e6,
+        "unit": "Mrays/s", "higher_is_better": True, "n_gpus": 1, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "Poisson arrivals 20/s (seed 5) of Cornell / instancing / volumes "
+                               "jobs, square 256..2048 px and 4..256 spp log-uniform, 64x64 "
+                               "tile-passes of 8 spp batched across jobs",
+                   "jobs": n, "arrival_rate_per_s": args.serve_rate,
+                   "max_jobs": sv.config.max_jobs,
+                   "iteration_paths": sv.config.iteration_paths},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "mean": float(np.mean(lat)), "max": float(np.max(lat))},
+        "queued_ms": {"p50": float(np.percentile(queued, 50)),
+                      "p99": float(np.percentile(queued, 99))},
+        "jobs_done": st.jobs_done, "jobs_failed": failed,
+        "wall_s": wall, "gpu_busy_s": st.busy_ms / 1e3,
+        "busy_mrays_per_s": st.rays / (st.busy_ms / 1e3) / 1e6 if st.busy_ms else None,
+        "samples_per_sec": st.paths / wall,
+        "offered_paths_per_s": paths_total / float(arrivals[-1] if n > 1 else 1.0),
+        "iterations": st.iterations, "scenes_resident_at_end": st.scenes_resident,
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.guiding:
         return run_guiding(args)
+    if args.serving:
+        return run_serving(args)
     return run_ours(args)
 
 

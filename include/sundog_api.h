@@ -355,4 +355,78 @@ SUNDOG_API int sundog_guide_outputs(const float* params, const float* queries, i
 SUNDOG_API int sundog_guide_gradients(const float* params, const float* records, int n,
                                       const float* box, float* grads, float* loss);
 
+/* ---- Render server (no counterpart in the reference) ----------------------
+ * Jobs (a scene, its size, spp and seed) are submitted from any thread. A
+ * server thread admits them in arrival order when a job slot and enough free
+ * device memory are available (jobs that fit pass one that does not), keeps
+ * each scene's device data (BVH, CDFs, textures, meshes) resident and shared
+ * by all jobs of that scene, and renders all admitted jobs together: each
+ * iteration is one persistent launch over tile-passes (a tile x tile pixel
+ * rectangle and a range of its samples) drawn from every active job, then one
+ * fold of those samples into each job's film. Jobs arriving while others run
+ * join at the next iteration. A job's film is bit-identical to a
+ * sundog_session_render of the same scene, size, spp and seed, alone or in
+ * any mix. */
+typedef struct sundog_server sundog_server;
+typedef struct {
+  int32_t max_jobs;            /* jobs on the device at once, 1..32 (16) */
+  int32_t tile;                /* tile edge in pixels, a multiple of 8 (64) */
+  int32_t pass_spp;            /* samples of a tile per tile-pass (8) */
+  int32_t reserved0;
+  uint64_t iteration_paths;    /* camera paths per launch (8388608) */
+  uint64_t reserve_bytes;      /* device memory left free at admission (1 GiB) */
+  uint64_t scene_cache_bytes;  /* scene data kept resident with no job using it (8 GiB) */
+} sundog_server_config;
+
+enum {
+  SUNDOG_JOB_QUEUED = 0,
+  SUNDOG_JOB_RUNNING = 1,
+  SUNDOG_JOB_DONE = 2,
+  SUNDOG_JOB_FAILED = 3,
+  SUNDOG_JOB_CANCELLED = 4
+};
+
+typedef struct {
+  int32_t state;               /* SUNDOG_JOB_* */
+  int32_t width, height, spp;
+  uint64_t paths_done, paths_total;
+  double queued_ms;            /* submission -> admission */
+  double latency_ms;           /* submission -> film on the host (final states) */
+  char error[256];             /* reason for FAILED */
+} sundog_job_status;
+
+typedef struct {
+  uint64_t jobs_submitted, jobs_done, jobs_failed, jobs_cancelled;
+  uint64_t iterations;         /* persistent launches */
+  uint64_t rays;               /* radiance + shadow traces of all jobs */
+  uint64_t paths;              /* camera paths of all jobs */
+  double busy_ms;              /* CUDA-event time of the iterations */
+  double wall_ms;              /* since sundog_server_create */
+  int32_t active_jobs, queued_jobs;
+  uint64_t scenes_resident;
+  uint64_t scene_bytes;        /* device memory held by resident scenes */
+} sundog_server_statistics;
+
+SUNDOG_API void sundog_server_defaults(sundog_server_config* config);
+/* config NULL = defaults. Returns NULL on error (sundog_last_error). */
+SUNDOG_API sundog_server* sundog_server_create(const sundog_server_config* config);
+/* Queues a render of the scene (copied: the handle may be destroyed after the
+ * call). options: width / height / spp / seed / transparent_shadows / clamp
+ * overrides as in sundog_render (NULL = the scene's). film_rgba: host buffer
+ * of width*height float4 receiving the film when the job is done (NULL = none;
+ * must stay valid until the job ends). Returns the job id, or -1. */
+SUNDOG_API int64_t sundog_server_submit(sundog_server*, sundog_scene*,
+                                        const sundog_render_options* options, float* film_rgba);
+SUNDOG_API int sundog_server_status(sundog_server*, int64_t job, sundog_job_status*);
+/* Waits until the job is DONE, FAILED or CANCELLED (timeout_ms < 0: no
+ * limit). Returns 0 when it is, 1 on timeout or error. */
+SUNDOG_API int sundog_server_wait(sundog_server*, int64_t job, double timeout_ms,
+                                  sundog_job_status*);
+/* Cancels a queued or running job (between iterations); its film is not
+ * written. Returns 0, or 1 if the job is unknown or already final. */
+SUNDOG_API int sundog_server_cancel(sundog_server*, int64_t job);
+SUNDOG_API int sundog_server_stats(sundog_server*, sundog_server_statistics*);
+/* Cancels what is left, stops the server thread, frees device memory. */
+SUNDOG_API void sundog_server_destroy(sundog_server*);
+
 #endif /* SUNDOG_B200_API_H */

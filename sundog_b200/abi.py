@@ -98,6 +98,33 @@ class GuidingStats(ctypes.Structure):
                 ("box_lo", ctypes.c_float * 3), ("box_hi", ctypes.c_float * 3)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("max_jobs", ctypes.c_int32), ("tile", ctypes.c_int32),
+                ("pass_spp", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+                ("iteration_paths", ctypes.c_uint64), ("reserve_bytes", ctypes.c_uint64),
+                ("scene_cache_bytes", ctypes.c_uint64)]
+
+
+class JobStatus(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32), ("spp", ctypes.c_int32),
+                ("paths_done", ctypes.c_uint64), ("paths_total", ctypes.c_uint64),
+                ("queued_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("error", ctypes.c_char * 256)]
+
+
+class ServerStatistics(ctypes.Structure):
+    _fields_ = [("jobs_submitted", ctypes.c_uint64), ("jobs_done", ctypes.c_uint64),
+                ("jobs_failed", ctypes.c_uint64), ("jobs_cancelled", ctypes.c_uint64),
+                ("iterations", ctypes.c_uint64), ("rays", ctypes.c_uint64),
+                ("paths", ctypes.c_uint64), ("busy_ms", ctypes.c_double),
+                ("wall_ms", ctypes.c_double), ("active_jobs", ctypes.c_int32),
+                ("queued_jobs", ctypes.c_int32), ("scenes_resident", ctypes.c_uint64),
+                ("scene_bytes", ctypes.c_uint64)]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = range(5)
+
 # Parameter count of the guiding network (include/sundog_api.h).
 GUIDE_PARAMS = 14576
 
@@ -124,7 +151,9 @@ ADDITIVE_SYMBOLS = [
     "sundog_session_render_tile_noalloc", "sundog_guiding_defaults",
     "sundog_session_set_guiding", "sundog_session_guiding_stats", "sundog_guide_init_params",
     "sundog_guide_outputs", "sundog_guide_gradients", "sundog_session_guide_params",
-    "sundog_session_guide_records",
+    "sundog_session_guide_records", "sundog_server_defaults", "sundog_server_create",
+    "sundog_server_submit", "sundog_server_status", "sundog_server_wait",
+    "sundog_server_cancel", "sundog_server_stats", "sundog_server_destroy",
 ]
 
 _lib = None
@@ -202,6 +231,18 @@ def load(path=None):
     lib.sundog_session_guide_params.argtypes = [vp, vp]
     lib.sundog_session_guide_records.argtypes = [vp, vp, ctypes.c_uint64,
                                                  ctypes.POINTER(ctypes.c_uint64)]
+    lib.sundog_server_defaults.argtypes = [ctypes.POINTER(ServerConfig)]
+    lib.sundog_server_defaults.restype = None
+    lib.sundog_server_create.argtypes = [ctypes.POINTER(ServerConfig)]
+    lib.sundog_server_create.restype = vp
+    lib.sundog_server_submit.argtypes = [vp, vp, ctypes.POINTER(RenderOptions), vp]
+    lib.sundog_server_submit.restype = ctypes.c_int64
+    lib.sundog_server_status.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(JobStatus)]
+    lib.sundog_server_wait.argtypes = [vp, ctypes.c_int64, dp, ctypes.POINTER(JobStatus)]
+    lib.sundog_server_cancel.argtypes = [vp, ctypes.c_int64]
+    lib.sundog_server_stats.argtypes = [vp, ctypes.POINTER(ServerStatistics)]
+    lib.sundog_server_destroy.argtypes = [vp]
+    lib.sundog_server_destroy.restype = None
     if path is None:
         _lib = lib
     return lib

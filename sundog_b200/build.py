@@ -23,7 +23,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 CU_SOURCES = ["pt_kernel.cu", "selftest.cu", "noalloc.cu", "guide.cu", "serve.cu"]
 CPP_SOURCES = ["scene_api.cpp", "scene_derive.cpp", "assets.cpp", "bvh_build.cpp",
-               "render.cpp", "render_api.cpp"]
+               "render.cpp", "render_api.cpp", "serve_host.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",

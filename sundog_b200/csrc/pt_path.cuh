@@ -58,20 +58,13 @@ __device__ __forceinline__ uint16_t medAt(unsigned long long med, int i) {
   return (uint16_t)((med >> (16 * i)) & 0xFFFFull);
 }
 
-// Camera sample for path index id; false if the index is tile padding.
-// (device/programs.cu:312-357)
-__device__ __forceinline__ bool startPath(const SdLaunch& lp, unsigned long long id, Path& p) {
-  int sLocal = (int)(id / (unsigned long long)lp.npixPad);
-  int rem = (int)(id - (unsigned long long)sLocal * lp.npixPad);
-  int tile = rem >> 6, within = rem & 63;
-  int tx = tile % lp.tilesX, ty = tile / lp.tilesX;
-  int px = tx * 8 + (within & 7), py = ty * 8 + (within >> 3);
-  if (px >= lp.width || py >= lp.height) return false;
+// Camera sample s of pixel (px, py): jittered (stratified while s < n^2)
+// position, thin-lens origin, initial path state. The random stream depends
+// only on (pixel, s, seed). (device/programs.cu:312-357)
+__device__ __forceinline__ void startPathAt(const SdLaunch& lp, int px, int py, int s, Path& p) {
   int pixel = py * lp.width + px;
-  int s = lp.sampleOffset + sLocal;
   p.pixel = pixel;
   p.s = s;
-  p.slot = sLocal * (lp.width * lp.height) + pixel;
   p.rng = Pcg::seeded(((unsigned long long)pixel << 32) ^ (unsigned long long)s,
                       (unsigned long long)lp.seed);
   int ns = lp.nStrata;
@@ -103,6 +96,18 @@ __device__ __forceinline__ bool startPath(const SdLaunch& lp, unsigned long long
   p.med = 0ull;
   p.medDepth = 0;
   p.depth = 0;
+}
+
+// Camera sample for path index id; false if the index is tile padding.
+__device__ __forceinline__ bool startPath(const SdLaunch& lp, unsigned long long id, Path& p) {
+  int sLocal = (int)(id / (unsigned long long)lp.npixPad);
+  int rem = (int)(id - (unsigned long long)sLocal * lp.npixPad);
+  int tile = rem >> 6, within = rem & 63;
+  int tx = tile % lp.tilesX, ty = tile / lp.tilesX;
+  int px = tx * 8 + (within & 7), py = ty * 8 + (within >> 3);
+  if (px >= lp.width || py >= lp.height) return false;
+  startPathAt(lp, px, py, lp.sampleOffset + sLocal, p);
+  p.slot = sLocal * (lp.width * lp.height) + py * lp.width + px;
   return true;
 }
 

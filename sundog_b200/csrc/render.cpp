@@ -157,44 +157,13 @@ RenderSession::~RenderSession() {
   if (kev[1]) cudaEventDestroy(kev[1]);
 }
 
-void RenderSession::build(const sundog_scene* h, const sundog_render_options* opt,
-                          const sundog_render_ext* ext) {
-  auto tTotal = Clock::now();
-  scene = h->scene;
-  quiet = opt && opt->quiet != 0;
-  // ---- overrides (src/capi_render.cpp:74-83) ----
-  RenderCfg& rs = scene.render;
-  if (opt) {
-    if (opt->spp > 0) rs.spp = opt->spp;
-    if (opt->width > 0) rs.width = opt->width;
-    if (opt->height > 0) rs.height = opt->height;
-    if (opt->seed >= 0) rs.seed = (unsigned)opt->seed;
-    if (opt->denoise >= 0) rs.denoise = opt->denoise == 1;
-    if (opt->transparent_shadows >= 0) rs.transparentShadows = opt->transparent_shadows == 1;
-    if (!std::isnan(opt->clamp) && opt->clamp >= 0.0) rs.clampVal = (float)opt->clamp;
-    float pt = std::isnan(opt->physics_time) ? -1.0f : (float)opt->physics_time;
-    if (pt >= 0.0f && !scene.physics.enabled)
-      throw std::runtime_error("--physics-time: scene has no physics block");
-  }
-  if (rs.width <= 0 || rs.height <= 0 || rs.spp <= 0) throw std::runtime_error("render: bad size");
-  if (scene.physics.enabled && !quiet)
-    std::fprintf(stderr,
-                 "sundog: physics settling is not part of this renderer; rendering authored "
-                 "poses\n");
-  aov = (opt && (opt->aov_albedo_path || opt->aov_normal_path)) ||
-        (ext && (ext->aov_albedo || ext->aov_normal));
-  int devId = 0;
-  cudaCheck(cudaGetDevice(&devId), "cudaGetDevice");
-  cudaCheck(cudaFree(nullptr), "CUDA context");
-  size_t freeB = 0, totB = 0;
-  cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
-  freeBefore = freeB;
-  cudaCheck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
-  cudaCheck(cudaEventCreate(&ev0), "event");
-  cudaCheck(cudaEventCreate(&ev1), "event");
-  cudaCheck(cudaEventCreate(&kev[0]), "event");
-  cudaCheck(cudaEventCreate(&kev[1]), "event");
-
+// Scene data on the device: assets, CDFs, BVH and uploads (the reference's
+// load-time steps, src/capi_render.cpp:84-221). Independent of the render
+// settings, so one copy serves every render of the scene.
+void DeviceScene::build(const SceneDesc& desc) {
+  scene = desc;
+  size_t freeB = 0, totB = 0, freeBefore = 0;
+  cudaCheck(cudaMemGetInfo(&freeBefore, &totB), "cudaMemGetInfo");
   // ---- assets ----
   auto tLoad = Clock::now();
   std::vector<HostMesh> meshes;
@@ -222,7 +191,7 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
     }
     texDescs.push_back(d);
   }
-  SdEnv env{};
+  env = SdEnv{};
   std::vector<float> envRgba;
   int envW = 0, envH = 0;
   if (scene.bgKind == BG_ENVMAP) {
@@ -407,6 +376,107 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
   dLights.upload(lights.data(), lights.size() * sizeof(SdLight));
   dFlames.upload(scene.flames.data(), scene.flames.size() * sizeof(SdFlame));
   buildMs = msSince(tBuild);
+  numLights = (int)lights.size();
+  numObjects = nObj;
+  wideNodes = wide;
+  cudaCheck(cudaDeviceSynchronize(), "scene upload");
+  cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
+  deviceBytes = freeBefore > freeB ? freeBefore - freeB : 0;
+}
+
+void DeviceScene::fillLaunch(SdLaunch& l) const {
+  l.bgKind = scene.bgKind;
+  l.bgA = scene.bgA;
+  l.bgB = scene.bgB;
+  l.env = env;
+  l.textures = (const SdTexture*)dTex.ptr;
+  l.materials = (const SdMaterial*)dMat.ptr;
+  l.lights = (const SdLight*)dLights.ptr;
+  l.numLights = numLights;
+  l.flames = (const SdFlame*)dFlames.ptr;
+  l.numFlames = (int)scene.flames.size();
+  l.nodes = wideNodes ? nullptr : (const BvhNode*)dNodes.ptr;
+  l.cw = wideNodes ? (const CwNode*)dNodes.ptr : nullptr;
+  l.tris = (const float4*)dTris.ptr;
+  l.inst = (const SdInstance*)dInst.ptr;
+  l.meshes = (const SdMesh*)dMeshes.ptr;
+  l.tlasRoot = 0;
+  l.numInstances = numObjects;
+}
+
+// Render settings and camera of one film (rs: settings after overrides).
+void fillRenderLaunch(SdLaunch& l, const SceneDesc& scene, const RenderCfg& rs) {
+  l.width = rs.width;
+  l.height = rs.height;
+  l.sppTotal = rs.spp;
+  l.maxDepth = rs.maxDepth;
+  l.nStrata = strataFor(rs.spp);
+  l.clampVal = rs.clampVal;
+  l.seed = rs.seed;
+  l.transparentShadows = rs.transparentShadows ? 1 : 0;
+  l.tilesX = (rs.width + 7) / 8;
+  l.npixPad = l.tilesX * ((rs.height + 7) / 8) * 64;
+  l.cam = buildCamera(scene.camera, rs.width, rs.height);
+}
+
+
+// Option overrides of sundog_render (src/capi_render.cpp:74-83).
+void applyRenderOverrides(SceneDesc& scene, const sundog_render_options* opt) {
+  RenderCfg& rs = scene.render;
+  if (opt) {
+    if (opt->spp > 0) rs.spp = opt->spp;
+    if (opt->width > 0) rs.width = opt->width;
+    if (opt->height > 0) rs.height = opt->height;
+    if (opt->seed >= 0) rs.seed = (unsigned)opt->seed;
+    if (opt->denoise >= 0) rs.denoise = opt->denoise == 1;
+    if (opt->transparent_shadows >= 0) rs.transparentShadows = opt->transparent_shadows == 1;
+    if (!std::isnan(opt->clamp) && opt->clamp >= 0.0) rs.clampVal = (float)opt->clamp;
+    float pt = std::isnan(opt->physics_time) ? -1.0f : (float)opt->physics_time;
+    if (pt >= 0.0f && !scene.physics.enabled)
+      throw std::runtime_error("--physics-time: scene has no physics block");
+  }
+  if (rs.width <= 0 || rs.height <= 0 || rs.spp <= 0) throw std::runtime_error("render: bad size");
+}
+
+void RenderSession::build(const sundog_scene* h, const sundog_render_options* opt,
+                          const sundog_render_ext* ext) {
+  auto tTotal = Clock::now();
+  scene = h->scene;
+  quiet = opt && opt->quiet != 0;
+  // ---- overrides (src/capi_render.cpp:74-83) ----
+  RenderCfg& rs = scene.render;
+  applyRenderOverrides(scene, opt);
+  if (scene.physics.enabled && !quiet)
+    std::fprintf(stderr,
+                 "sundog: physics settling is not part of this renderer; rendering authored "
+                 "poses\n");
+  aov = (opt && (opt->aov_albedo_path || opt->aov_normal_path)) ||
+        (ext && (ext->aov_albedo || ext->aov_normal));
+  int devId = 0;
+  cudaCheck(cudaGetDevice(&devId), "cudaGetDevice");
+  cudaCheck(cudaFree(nullptr), "CUDA context");
+  size_t freeB = 0, totB = 0;
+  cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
+  freeBefore = freeB;
+  cudaCheck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+  cudaCheck(cudaEventCreate(&ev0), "event");
+  cudaCheck(cudaEventCreate(&ev1), "event");
+  cudaCheck(cudaEventCreate(&kev[0]), "event");
+  cudaCheck(cudaEventCreate(&kev[1]), "event");
+
+  // ---- scene data (assets, CDFs, BVH, uploads) ----
+  {
+    std::shared_ptr<DeviceScene> ds(new DeviceScene());
+    ds->build(scene);
+    dev = ds;
+  }
+  loadMs = dev->loadMs;
+  buildMs = dev->buildMs;
+  meshTriangles = dev->meshTriangles;
+  numNodes = dev->numNodes;
+  numTris = dev->numTris;
+  tlasDepth = dev->tlasDepth;
+  blasDepth = dev->blasDepth;
 
   // ---- film and per-sample buffers ----
   size_t npix = (size_t)rs.width * rs.height;
@@ -433,18 +503,9 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
 
   SdLaunch& l = lp;
   std::memset(&l, 0, sizeof l);
-  l.width = rs.width;
-  l.height = rs.height;
-  l.sppTotal = rs.spp;
-  l.maxDepth = rs.maxDepth;
-  l.nStrata = strataFor(rs.spp);
-  l.clampVal = rs.clampVal;
-  l.seed = rs.seed;
-  l.transparentShadows = rs.transparentShadows ? 1 : 0;
+  fillRenderLaunch(l, scene, rs);
+  dev->fillLaunch(l);
   l.aovOn = aov ? 1 : 0;
-  l.tilesX = (rs.width + 7) / 8;
-  int tilesY = (rs.height + 7) / 8;
-  l.npixPad = l.tilesX * tilesY * 64;
   l.pathCounter = (unsigned long long*)counters.ptr;
   l.rayCounter = (unsigned long long*)counters.ptr + 1;
   l.sampleL = (float4*)sampleL.ptr;
@@ -453,24 +514,6 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
   l.accum = (float4*)accum.ptr;
   l.aovAlbedo = (float4*)aovAlb.ptr;
   l.aovNormal = (float4*)aovNrm.ptr;
-  l.cam = buildCamera(scene.camera, rs.width, rs.height);
-  l.bgKind = scene.bgKind;
-  l.bgA = scene.bgA;
-  l.bgB = scene.bgB;
-  l.env = env;
-  l.textures = (const SdTexture*)dTex.ptr;
-  l.materials = (const SdMaterial*)dMat.ptr;
-  l.lights = (const SdLight*)dLights.ptr;
-  l.numLights = (int)lights.size();
-  l.flames = (const SdFlame*)dFlames.ptr;
-  l.numFlames = (int)scene.flames.size();
-  l.nodes = wide ? nullptr : (const BvhNode*)dNodes.ptr;
-  l.cw = wide ? (const CwNode*)dNodes.ptr : nullptr;
-  l.tris = (const float4*)dTris.ptr;
-  l.inst = (const SdInstance*)dInst.ptr;
-  l.meshes = (const SdMesh*)dMeshes.ptr;
-  l.tlasRoot = 0;
-  l.numInstances = nObj;
   grid = renderGridSize();
   if (ext && ext->guiding) setGuiding(true, nullptr);
   cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");

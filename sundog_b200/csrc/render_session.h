@@ -42,6 +42,33 @@ void quadricBoundsHost(int kind, float3& lo, float3& hi);
 
 struct GuideState;  // guide.h
 
+// A scene's data on the device (textures, meshes, light CDFs, environment
+// CDFs, BVH, materials). Independent of resolution, spp and seed: several
+// films can render from one copy.
+struct DeviceScene {
+  SceneDesc scene;
+  SdEnv env{};
+  int numLights = 0, numObjects = 0;
+  bool wideNodes = false;
+  size_t meshTriangles = 0, numNodes = 0, numTris = 0, deviceBytes = 0;
+  int tlasDepth = 0, blasDepth = 0;
+  double loadMs = 0, buildMs = 0;
+  DevBuf envTex, envMarg, envCond;
+  std::vector<DevBuf> texImages;
+  std::vector<MeshBufs> meshBufs;
+  std::vector<DevBuf> lightBufs;
+  DevBuf dNodes, dTris, dInst, dMeshes, dTex, dMat, dLights, dFlames;
+
+  void build(const SceneDesc& desc);
+  void fillLaunch(SdLaunch& l) const;  // scene pointers and counts
+};
+
+// sundog_render's option overrides applied to a scene's render settings.
+void applyRenderOverrides(SceneDesc& scene, const sundog_render_options* opt);
+
+// Render settings and camera of one film of the given size.
+void fillRenderLaunch(SdLaunch& l, const SceneDesc& scene, const RenderCfg& rs);
+
 struct RenderSession {
   SceneDesc scene;
   SdLaunch lp{};
@@ -60,11 +87,7 @@ struct RenderSession {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t kev[2] = {nullptr, nullptr};  // around each path-kernel launch
 
-  DevBuf envTex, envMarg, envCond;
-  std::vector<DevBuf> texImages;
-  std::vector<MeshBufs> meshBufs;
-  std::vector<DevBuf> lightBufs;
-  DevBuf dNodes, dTris, dInst, dMeshes, dTex, dMat, dLights, dFlames;
+  std::shared_ptr<const DeviceScene> dev;
   DevBuf accum, aovAlb, aovNrm, sampleL, sampleAlb, sampleNrm, counters;
   std::unique_ptr<GuideState> guide;  // learned path guiding, when enabled
 
