@@ -144,13 +144,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_launch():
-    """DRAM bytes per path-kernel launch from the committed ncu summary."""
+def ncu_traffic_per_path():
+    """DRAM bytes (read + write) per camera path of the path kernel, from the
+    committed ncu summary of a smaller launch of the same workload (traffic
+    is per-path work: the per-sample radiance write and evicted stack
+    lines), so a launch's traffic is this times its paths."""
     p = os.path.join(ROOT, "profiles", "pt_persistent_instancing.md")
     if not os.path.isfile(p):
         return None
     with open(p) as f:
-        m = re.search(r"dram_bytes_per_full_launch:\s*([0-9.eE+]+)", f.read())
+        m = re.search(r"dram_bytes_per_path:\s*([0-9.eE+]+)", f.read())
     return float(m.group(1)) if m else None
 
 
@@ -222,6 +225,28 @@ def run_reference(args):
     return 0
 
 
+# ---- ranks ---------------------------------------------------------------------------------
+
+def sample_block(rank, spp):
+    """Samples [first, first + count) of the frame that `rank` renders: each
+    rank a disjoint block of spp samples (weak scaling, no data-path
+    collective; the blocks' films are independent estimates of one image,
+    averaged with equal weights)."""
+    return rank * spp, spp
+
+
+def reduce_max_sum(dist, device, t_max, *sums):
+    """Whole-job figures over ranks: the slowest rank's time, summed counts."""
+    if dist is None:
+        return (t_max,) + tuple(float(x) for x in sums)
+    import torch
+    t = torch.tensor([float(t_max)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(x) for x in sums], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return (float(t.item()),) + tuple(float(x) for x in c.tolist())
+
+
 # ---- our arm ------------------------------------------------------------------------------
 
 def run_ours(args):
@@ -245,7 +270,7 @@ def run_ours(args):
 
     scene = make_scene(args)
     base = asset_dir()
-    offset = rank * args.spp
+    offset, _ = sample_block(rank, args.spp)
     ses = sc.Session(scene, base_dir=base, sample_offset=offset)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -275,18 +300,46 @@ def run_ours(args):
     torch.cuda.synchronize()
     wall = time.perf_counter() - t_wall
     clk = clocks.stop()
-    total_ms = float(sum(step_ms))
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        r = torch.tensor([float(rays)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(r, op=dist.ReduceOp.SUM)
-        rays_all = float(r.item())
-        dist.barrier()
-    else:
-        rays_all = float(rays)
+    total_ms, rays_all = reduce_max_sum(dist, "cuda", float(sum(step_ms)), rays)
     value = rays_all / (total_ms / 1000.0) / 1e6
+
+    # End to end through the public API with host buffers, every rank its
+    # own sample block (asset load, CDF + BVH build, upload, render, film
+    # download inside the timed call); whole job = slowest rank, summed rays.
+    e2e = None
+    if not args.no_e2e:
+        h = scene.build(base, lib)
+        try:
+            film = np.zeros((args.height, args.width, 4), np.float32)
+            o = abi.options(quiet=True)
+            ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, offset)
+            rr = abi.RenderResult()
+            abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
+                                           ctypes.byref(rr)), "render_ex", lib)  # warm
+            h0, d0 = ctypes.c_uint64(), ctypes.c_uint64()
+            lib.sundog_transfer_bytes(ctypes.byref(h0), ctypes.byref(d0))
+            e_steps = max(1, min(args.steps, 3))
+            if dist:
+                dist.barrier()
+            t0 = time.perf_counter()
+            erays = 0
+            for _ in range(e_steps):
+                abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
+                                               ctypes.byref(rr)), "render_ex", lib)
+                erays += rr.rays_traced
+            et = time.perf_counter() - t0
+            h1, d1 = ctypes.c_uint64(), ctypes.c_uint64()
+            lib.sundog_transfer_bytes(ctypes.byref(h1), ctypes.byref(d1))
+        finally:
+            lib.sundog_scene_destroy(h)
+        et, erays, hb, db = reduce_max_sum(dist, "cuda", et, erays, h1.value - h0.value,
+                                           d1.value - d0.value)
+        e2e = {"value": erays / et / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": int(hb / e_steps),
+               "d2h_bytes_per_step": int(db / e_steps),
+               "ms_per_step": 1000.0 * et / e_steps,
+               "path": "sundog_render_ex per rank: OBJ/HDR load, CDF + BVH build, upload, "
+                       "render, film download; slowest rank"}
 
     line = None
     if rank == 0:
@@ -300,10 +353,9 @@ def run_ours(args):
         rays_per_launch = rays / (args.steps * kernel_launches)
         achieved = bpr * rays_per_launch / (mean_launch_ms / 1000.0) / 1e9
         peak, peak_kind = measured_peaks()
-        traffic = ncu_traffic_per_launch()
-        if traffic is not None:
-            # the summary is per full-frame render; spread over this run's launches
-            traffic = traffic / kernel_launches
+        per_path = ncu_traffic_per_path()
+        paths_per_launch = args.width * args.height * args.spp / kernel_launches
+        traffic = per_path * paths_per_launch if per_path is not None else None
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "traffic": traffic,
                     "peak_source": peak_kind,
@@ -319,37 +371,6 @@ def run_ours(args):
                             "quadric, 64 B/instance) per path-kernel launch over its CUDA-event "
                             "duration; the BVH (<4 MB) and env tables are L2-resident, so HBM "
                             "is a loose bound"}
-        e2e = None
-        if not args.no_e2e:
-            h = scene.build(base, lib)
-            try:
-                npix = args.width * args.height
-                film = np.zeros((args.height, args.width, 4), np.float32)
-                o = abi.options(quiet=True)
-                ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, offset)
-                rr = abi.RenderResult()
-                abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
-                                               ctypes.byref(rr)), "render_ex", lib)  # warm
-                h0, d0 = ctypes.c_uint64(), ctypes.c_uint64()
-                lib.sundog_transfer_bytes(ctypes.byref(h0), ctypes.byref(d0))
-                e_steps = max(1, min(args.steps, 3))
-                t0 = time.perf_counter()
-                erays = 0
-                for _ in range(e_steps):
-                    abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
-                                                   ctypes.byref(rr)), "render_ex", lib)
-                    erays += rr.rays_traced
-                et = time.perf_counter() - t0
-                h1, d1 = ctypes.c_uint64(), ctypes.c_uint64()
-                lib.sundog_transfer_bytes(ctypes.byref(h1), ctypes.byref(d1))
-                e2e = {"value": erays / et / 1e6, "unit": UNIT,
-                       "h2d_bytes_per_step": int((h1.value - h0.value) / e_steps),
-                       "d2h_bytes_per_step": int((d1.value - d0.value) / e_steps),
-                       "ms_per_step": 1000.0 * et / e_steps,
-                       "path": "sundog_render_ex: OBJ/HDR load, CDF + BVH build, upload, "
-                               "render, film download"}
-            finally:
-                lib.sundog_scene_destroy(h)
         cpu = None
         if not args.no_cpu_baseline:
             cpu, _, _ = oracle_sample(scene, base, args, args.cpu_seconds, os.cpu_count() or 1)
@@ -361,7 +382,7 @@ def run_ours(args):
                            "spp": args.spp, "paths_per_step": args.width * args.height * args.spp,
                            "l2": "flushed between steps (256 MiB write); BVH + env tables "
                                  "re-fetched each step",
-                           "parallelism": "dp%d (rank r renders samples [64r, 64r+64))" % world,
+                           "parallelism": "dp%d (rank r renders samples [spp r, spp (r+1)))" % world,
                            "grid": st.grid, "block": st.block, "chunk_spp": st.chunk_spp},
                 "samples_per_sec": args.width * args.height * args.spp * world /
                                    (total_ms / 1000.0 / args.steps) if total_ms else None,

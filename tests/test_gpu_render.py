@@ -142,3 +142,27 @@ def test_session_matches_render(lib, asset_dir):
         f2 = ses.read()
     assert f1.tobytes() == film.tobytes() == f2.tobytes()
     assert r1.rays_traced == r2.rays_traced > 0
+
+
+def test_sample_blocks_combine(lib, asset_dir):
+    """The multi-GPU decomposition: rank r renders samples [spp r, spp (r+1))
+    of the same frame (sample_offset). A film that folds samples
+    [s0, s0 + n) into an empty film by the running mean holds their sum over
+    (s0 + n), so the full estimate is sum_r film_r (s0_r + n_r) / N. Two
+    8-sample blocks rendered apart combine into the 16-sample render up to
+    FP32 rounding (every sample is the same sample in both)."""
+    s16 = workloads.instancing(asset_dir, width=64, height=48, spp=16)
+    s8 = workloads.instancing(asset_dir, width=64, height=48, spp=8)
+    with sc.Session(s16, base_dir=asset_dir) as ses:
+        ses.render()
+        full = ses.read()[..., :3].astype(np.float64)
+    blocks = []
+    for first in (0, 8):
+        with sc.Session(s8, base_dir=asset_dir, sample_offset=first) as ses:
+            ses.render()
+            blocks.append(ses.read()[..., :3].astype(np.float64))
+    comb = (blocks[0] * 8 + blocks[1] * 16) / 16.0
+    err = np.abs(comb - full) / np.maximum(np.abs(full), 1e-3)
+    print("sample blocks: max rel diff %.2e" % err.max())
+    assert err.max() <= 1e-4
+    assert not np.array_equal(blocks[0], blocks[1])
