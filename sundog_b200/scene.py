@@ -318,14 +318,14 @@ class Session(object):
     """A scene resident on the device (sundog_session_*)."""
 
     def __init__(self, scene, base_dir=".", aov=False, chunk_spp=0, guiding=0, sample_offset=0,
-                 **opts):
+                 frame_spp=0, **opts):
         self.lib = abi.load()
         h = scene.build(base_dir, self.lib)
         try:
             o = abi.options(**opts)
             dummy = np.zeros(4, np.float32)
             ext = abi.RenderExt(None, dummy.ctypes.data if aov else None, None, chunk_spp, 1,
-                                guiding, sample_offset)
+                                guiding, sample_offset, frame_spp)
             self.handle = self.lib.sundog_session_create(h, ctypes.byref(o), ctypes.byref(ext))
             if not self.handle:
                 raise abi.SundogError("session: " + abi.last_error(self.lib))

@@ -146,11 +146,12 @@ def test_session_matches_render(lib, asset_dir):
 
 def test_sample_blocks_combine(lib, asset_dir):
     """The multi-GPU decomposition: rank r renders samples [spp r, spp (r+1))
-    of the same frame (sample_offset). A film that folds samples
-    [s0, s0 + n) into an empty film by the running mean holds their sum over
-    (s0 + n), so the full estimate is sum_r film_r (s0_r + n_r) / N. Two
-    8-sample blocks rendered apart combine into the 16-sample render up to
-    FP32 rounding (every sample is the same sample in both)."""
+    of the same frame (sample_offset, with frame_spp = the frame's samples so
+    the pixel strata are the frame's). A film that folds samples [s0, s0 + n)
+    into an empty film by the running mean holds their sum over (s0 + n), so
+    the full estimate is sum_r film_r (s0_r + n_r) / N. Two 8-sample blocks
+    rendered apart combine into the 16-sample render up to FP32 rounding
+    (every sample is the same sample in both)."""
     s16 = workloads.instancing(asset_dir, width=64, height=48, spp=16)
     s8 = workloads.instancing(asset_dir, width=64, height=48, spp=8)
     with sc.Session(s16, base_dir=asset_dir) as ses:
@@ -158,7 +159,7 @@ def test_sample_blocks_combine(lib, asset_dir):
         full = ses.read()[..., :3].astype(np.float64)
     blocks = []
     for first in (0, 8):
-        with sc.Session(s8, base_dir=asset_dir, sample_offset=first) as ses:
+        with sc.Session(s8, base_dir=asset_dir, sample_offset=first, frame_spp=16) as ses:
             ses.render()
             blocks.append(ses.read()[..., :3].astype(np.float64))
     comb = (blocks[0] * 8 + blocks[1] * 16) / 16.0
