@@ -59,6 +59,8 @@ def parse_args():
                     help="target CPU time of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--engine", type=int, default=0, choices=[0, 1, 2],
+                    help="path-tracing kernels: 0 automatic, 1 megakernel, 2 wavefront")
     ap.add_argument("--guiding", action="store_true",
                     help="learned-guiding equal-time relMSE line instead of Mrays/s")
     ap.add_argument("--guide-spp", type=int, default=256)
@@ -271,7 +273,8 @@ def run_ours(args):
     scene = make_scene(args)
     base = asset_dir()
     offset, _ = sample_block(rank, args.spp)
-    ses = sc.Session(scene, base_dir=base, sample_offset=offset, frame_spp=args.spp * world)
+    ses = sc.Session(scene, base_dir=base, sample_offset=offset, frame_spp=args.spp * world,
+                     engine=args.engine)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -312,7 +315,8 @@ def run_ours(args):
         try:
             film = np.zeros((args.height, args.width, 4), np.float32)
             o = abi.options(quiet=True)
-            ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, offset, args.spp * world)
+            ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, offset, args.spp * world,
+                                args.engine)
             rr = abi.RenderResult()
             abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
                                            ctypes.byref(rr)), "render_ex", lib)  # warm
@@ -383,7 +387,9 @@ def run_ours(args):
                            "l2": "flushed between steps (256 MiB write); BVH + env tables "
                                  "re-fetched each step",
                            "parallelism": "dp%d (rank r renders samples [spp r, spp (r+1)))" % world,
-                           "grid": st.grid, "block": st.block, "chunk_spp": st.chunk_spp},
+                           "grid": st.grid, "block": st.block, "chunk_spp": st.chunk_spp,
+                           "engine": ["automatic (wavefront)", "megakernel",
+                                      "wavefront"][args.engine]},
                 "samples_per_sec": args.width * args.height * args.spp * world /
                                    (total_ms / 1000.0 / args.steps) if total_ms else None,
                 "wall_s": wall,

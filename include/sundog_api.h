@@ -199,6 +199,10 @@ typedef struct {
                             of: the pixel strata follow it, so blocks rendered
                             apart (one per GPU) hold exactly the frame's
                             samples; <= 0 = this render's spp */
+  int32_t engine;        /* path-tracing kernels: 0 = automatic (wavefront for
+                            plain renders, megakernel for guided ones), 1 =
+                            persistent megakernel, 2 = wavefront (plain renders
+                            only). Both give the same samples. */
 } sundog_render_ext;
 
 typedef struct {
@@ -369,8 +373,8 @@ SUNDOG_API int sundog_guide_gradients(const float* params, const float* records,
  * rectangle and a range of its samples) drawn from every active job, then one
  * fold of those samples into each job's film. Jobs arriving while others run
  * join at the next iteration. A job's film is bit-identical to a
- * sundog_session_render of the same scene, size, spp and seed, alone or in
- * any mix. */
+ * sundog_session_render of the same scene, size, spp and seed with the
+ * megakernel engine (sundog_render_ext.engine = 1), alone or in any mix. */
 typedef struct sundog_server sundog_server;
 typedef struct {
   int32_t max_jobs;            /* jobs on the device at once, 1..32 (16) */

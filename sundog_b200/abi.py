@@ -54,7 +54,8 @@ class RenderExt(ctypes.Structure):
     _fields_ = [("film_rgba", ctypes.c_void_p), ("aov_albedo", ctypes.c_void_p),
                 ("aov_normal", ctypes.c_void_p), ("chunk_spp", ctypes.c_int32),
                 ("repeat", ctypes.c_int32), ("guiding", ctypes.c_int32),
-                ("sample_offset", ctypes.c_int32), ("frame_spp", ctypes.c_int32)]
+                ("sample_offset", ctypes.c_int32), ("frame_spp", ctypes.c_int32),
+                ("engine", ctypes.c_int32)]
 
 
 class RenderResult(ctypes.Structure):

@@ -25,6 +25,7 @@
 #include "guide.h"
 #include "kernels.h"
 #include "render_session.h"
+#include "wavefront.h"
 #include "scene_model.h"
 
 using namespace sdb;
@@ -150,6 +151,7 @@ static int strataFor(int spp) {  // device/programs.cu:317-319
 }
 
 RenderSession::~RenderSession() {
+  wf.reset();
   if (stream) cudaStreamDestroy(stream);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
@@ -505,6 +507,8 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
   std::memset(&l, 0, sizeof l);
   fillRenderLaunch(l, scene, rs);
   if (ext && ext->frame_spp > 0) l.nStrata = strataFor(ext->frame_spp);
+  engine = ext ? ext->engine : 0;
+  if (engine < 0 || engine > 2) throw std::runtime_error("render: engine must be 0, 1 or 2");
   dev->fillLaunch(l);
   l.aovOn = aov ? 1 : 0;
   l.pathCounter = (unsigned long long*)counters.ptr;
@@ -521,6 +525,12 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
   deviceBytes = freeBefore > freeB ? freeBefore - freeB : 0;
   setupMs = msSince(tTotal);
 }
+
+// Wavefront pool size (slots): 4 M (about 1.3 GB) keeps every stage launch full.
+#ifndef SDB_WF_SLOTS_LOG2
+#define SDB_WF_SLOTS_LOG2 22
+#endif
+static constexpr unsigned long long kWavefrontSlots = 1ull << SDB_WF_SLOTS_LOG2;
 
 void RenderSession::setGuiding(bool enable, const sundog_guiding_config* cfg) {
   if (!enable) {
@@ -563,14 +573,22 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
     cudaCheck(cudaMemsetAsync(lp.pathCounter, 0, sizeof(unsigned long long), st), "counter reset");
     cudaCheck(setLaunch(lp, st), "launch params");
     cudaCheck(cudaEventRecord(kev[0], st), "event");
-    cudaCheck(launchRender(st, grid, mode), "path kernel launch");
+    const bool wavefront = mode == 0 && engine != 1;
+    if (wavefront) {
+      if (!wf) wf.reset(new WfBuffers());
+      wf->ensure((int)std::min<unsigned long long>(lp.numPaths, kWavefrontSlots));
+      launches += wfRender(lp, *wf, st);
+    } else {
+      cudaCheck(launchRender(st, grid, mode), "path kernel launch");
+      launches += 1;
+    }
     cudaCheck(cudaEventRecord(kev[1], st), "event");
     cudaCheck(cudaEventSynchronize(kev[1]), "path kernel");
     float one = 0.0f;
     cudaCheck(cudaEventElapsedTime(&one, kev[0], kev[1]), "event time");
     kms += one;
     cudaCheck(launchFold((int)npix, st), "fold launch");
-    launches += 2;
+    launches += 1;
     done += n;
     if (mode & kGuideRecord) {
       guide->trainAndBake(lp, st, n);

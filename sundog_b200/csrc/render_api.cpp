@@ -19,6 +19,7 @@
 #include "abi_util.h"
 #include "guide.h"
 #include "render_session.h"
+#include "wavefront.h"
 
 using namespace sdb;
 

@@ -41,6 +41,7 @@ void buildMeshLightCdf(const std::vector<float3>& wp, const std::vector<uint3>& 
 void quadricBoundsHost(int kind, float3& lo, float3& hi);
 
 struct GuideState;  // guide.h
+struct WfBuffers;   // wavefront.h
 
 // A scene's data on the device (textures, meshes, light CDFs, environment
 // CDFs, BVH, materials). Independent of resolution, spp and seed: several
@@ -90,6 +91,8 @@ struct RenderSession {
   std::shared_ptr<const DeviceScene> dev;
   DevBuf accum, aovAlb, aovNrm, sampleL, sampleAlb, sampleNrm, counters;
   std::unique_ptr<GuideState> guide;  // learned path guiding, when enabled
+  std::unique_ptr<WfBuffers> wf;      // wavefront slot pool, when used
+  int engine = 0;                     // sundog_render_ext.engine
 
   ~RenderSession();
   void build(const sundog_scene* h, const sundog_render_options* opt, const sundog_render_ext* ext);

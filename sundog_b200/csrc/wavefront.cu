@@ -1,0 +1,261 @@
+// Wavefront path tracer: the plain path kernel's per-path computation split
+// into stages over a pool of path slots held in global memory.
+//
+//   wfStart    fill every slot with a camera path
+//   per iteration, over the slots in the live list:
+//   wfTrace    trace the radiance ray (traversal only)
+//   wfShadeA   shadeVertex: media, flames, escape, shading, emission, the NEE
+//              light draw; queues the slot's shadow ray
+//   wfShadow   trace the queued shadow rays (transparent-shadow traversal)
+//   wfShadeB   finishVertex: NEE contribution, BSDF sample, roulette
+//
+// A slot whose path ends writes that sample and takes the next camera path at
+// once (warp-aggregated counter), so the pool stays full until the frame's
+// paths run out. Each stage's code is small next to the megakernel's and
+// keeps its state in registers instead of a 1 KB spilled frame, so at full
+// occupancy the instruction and local-memory traffic of the megakernel
+// disappear; the price is the path state's round trip through global memory
+// between stages (a few hundred bytes per path segment).
+//
+// The stages call the megakernel's own shadeVertex / finishVertex /
+// traverse in the same order with the same random draws, so every sample is
+// the same sample as in ptPersistent, and the film fold is unchanged.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <stdexcept>
+
+#include "pt_path.cuh"
+#include "wavefront.h"
+
+namespace sdb {
+
+namespace cg = cooperative_groups;
+
+__constant__ SdLaunch c_wlp;
+__constant__ WfPool c_pool;
+
+#ifndef SDB_WF_TRACE_BLOCKS
+#define SDB_WF_TRACE_BLOCKS 8
+#endif
+// Resident blocks per SM the stage kernels are compiled for (measured on the
+// instancing frame: traversal 8 -> 64 registers; shading 4 -> 128 registers,
+// 871 Mrays/s against 807-861 for 12/16 traversal or 8/16 shading blocks).
+#ifndef SDB_WF_SHADE_BLOCKS
+#define SDB_WF_SHADE_BLOCKS 4
+#endif
+
+// Slot index for an append to a list by the calling lanes together.
+__device__ __forceinline__ unsigned appendSlot(unsigned* count) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  unsigned base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(count, g.size());
+  return g.shfl(base, 0) + g.thread_rank();
+}
+
+__device__ __forceinline__ unsigned long long nextPathId() {
+  cg::coalesced_group g = cg::coalesced_threads();
+  unsigned long long base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(c_wlp.pathCounter, (unsigned long long)g.size());
+  return g.shfl(base, 0) + g.thread_rank();
+}
+
+// Puts the next camera path in `slot` and lists it in list `out`; leaves the
+// slot empty when the frame's paths are used up.
+__device__ __forceinline__ void refill(int slot, int out) {
+  const SdLaunch& lp = c_wlp;
+  const WfPool& pool = c_pool;
+  while (true) {
+    unsigned long long id = nextPathId();
+    if (id >= lp.numPaths) return;
+    Path p;
+    if (startPath(lp, id, p)) {
+      pool.paths[slot] = p;
+      pool.lists[out][appendSlot(&pool.counts[out])] = slot;
+      return;
+    }
+  }
+}
+
+__device__ __forceinline__ void finishPath(const Path& p) {
+  float3 L = sanitize3(p.L);
+  c_wlp.sampleL[p.slot] = make_float4(L.x, L.y, L.z, 1.0f);
+}
+
+__device__ __forceinline__ void addRays(unsigned long long rays) {
+  for (int off = 16; off > 0; off >>= 1) rays += __shfl_down_sync(0xFFFFFFFFu, rays, off);
+  if ((threadIdx.x & 31) == 0 && rays) atomicAdd(c_wlp.rayCounter, rays);
+}
+
+__global__ void __launch_bounds__(kRenderBlock) wfStart() {
+  const WfPool& pool = c_pool;
+  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < pool.cap;
+       slot += gridDim.x * blockDim.x)
+    refill(slot, 0);
+}
+
+__global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTrace(int in) {
+  const SdLaunch& lp = c_wlp;
+  const WfPool& pool = c_pool;
+  const unsigned n = pool.counts[in];
+  unsigned long long rays = 0;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int slot = pool.lists[in][i];
+    const Path& p = pool.paths[slot];
+    TraceHit h;
+    float dummyTr = 1.0f;
+    float3 dummyTau = v3(0.0f);
+    bool hit = traverse<false, false>(lp, p.o, p.d, 1e16f, h, dummyTr, dummyTau, nullptr);
+    if (!hit) h.inst = -1;
+    pool.hits[slot] = h;
+    rays++;
+  }
+  addRays(rays);
+}
+
+__global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeA(int in, int out) {
+  const SdLaunch& lp = c_wlp;
+  const WfPool& pool = c_pool;
+  const unsigned n = pool.counts[in];
+  unsigned long long rays = 0;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int slot = pool.lists[in][i];
+    Path p = pool.paths[slot];
+    TraceHit h = pool.hits[slot];
+    Vertex v;
+    if (shadeVertex<false>(lp, p, h.inst >= 0, h, rays, v)) {
+      pool.paths[slot] = p;
+      pool.verts[slot] = v;
+      pool.pending[slot] = 1;
+      if (v.nee) pool.shadowList[appendSlot(&pool.counts[2])] = slot;
+    } else {
+      finishPath(p);
+      pool.pending[slot] = 0;
+      refill(slot, out);
+    }
+  }
+  addRays(rays);
+}
+
+__global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfShadow() {
+  const SdLaunch& lp = c_wlp;
+  const WfPool& pool = c_pool;
+  const unsigned n = pool.counts[2];
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int slot = pool.shadowList[i];
+    const Vertex& v = pool.verts[slot];
+    float3 tr = shadowTransmittance<false>(lp, v.so, v.wi, v.tmaxS, nullptr);
+    pool.trs[slot] = make_float4(tr.x, tr.y, tr.z, 0.0f);
+  }
+}
+
+__global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeB(int in, int out) {
+  const SdLaunch& lp = c_wlp;
+  const WfPool& pool = c_pool;
+  const unsigned n = pool.counts[in];
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int slot = pool.lists[in][i];
+    if (!pool.pending[slot]) continue;
+    Path p = pool.paths[slot];
+    const Vertex v = pool.verts[slot];
+    float3 tr = v3(0.0f);
+    if (v.nee) {
+      float4 t4 = pool.trs[slot];
+      tr = v3(t4.x, t4.y, t4.z);
+    }
+    if (finishVertex<0>(lp, p, v, tr)) {
+      pool.paths[slot] = p;
+      pool.lists[out][appendSlot(&pool.counts[out])] = slot;
+    } else {
+      finishPath(p);
+      refill(slot, out);
+    }
+  }
+}
+
+// ---- host ---------------------------------------------------------------------
+
+template <typename K>
+static int gridFor(K kernel) {
+  int dev = 0, sms = 0, perSm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kRenderBlock, 0);
+  return sms * (perSm < 1 ? 1 : perSm);
+}
+
+void WfBuffers::ensure(int slots) {
+  if (slots <= cap) return;
+  paths.alloc((size_t)slots * sizeof(Path));
+  verts.alloc((size_t)slots * sizeof(Vertex));
+  hits.alloc((size_t)slots * sizeof(TraceHit));
+  trs.alloc((size_t)slots * sizeof(float4));
+  pending.alloc((size_t)slots);
+  list0.alloc((size_t)slots * sizeof(int));
+  list1.alloc((size_t)slots * sizeof(int));
+  shadow.alloc((size_t)slots * sizeof(int));
+  if (!counts.ptr) counts.alloc(4 * sizeof(unsigned));
+  if (!hostCount) cudaCheck(cudaMallocHost((void**)&hostCount, sizeof(unsigned)), "pinned count");
+  cap = slots;
+  gridTrace = gridFor(wfTrace);
+  gridShadeA = gridFor(wfShadeA);
+  gridShadow = gridFor(wfShadow);
+  gridShadeB = gridFor(wfShadeB);
+  gridStart = gridFor(wfStart);
+}
+
+WfBuffers::~WfBuffers() {
+  if (hostCount) cudaFreeHost(hostCount);
+}
+
+size_t wfSlotBytes() {
+  return sizeof(Path) + sizeof(Vertex) + sizeof(TraceHit) + sizeof(float4) + 1 + 3 * sizeof(int);
+}
+
+// Renders the launch block's paths (lp.numPaths ids, counters already
+// cleared) into lp.sampleL through the stages. Returns the kernels launched.
+int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st) {
+  WfPool pool;
+  pool.paths = (Path*)b.paths.ptr;
+  pool.verts = (Vertex*)b.verts.ptr;
+  pool.hits = (TraceHit*)b.hits.ptr;
+  pool.trs = (float4*)b.trs.ptr;
+  pool.pending = (unsigned char*)b.pending.ptr;
+  pool.lists[0] = (int*)b.list0.ptr;
+  pool.lists[1] = (int*)b.list1.ptr;
+  pool.shadowList = (int*)b.shadow.ptr;
+  pool.counts = (unsigned*)b.counts.ptr;
+  pool.cap = (int)std::min<unsigned long long>((unsigned long long)b.cap, lp.numPaths);
+  cudaCheck(cudaMemcpyToSymbolAsync(c_wlp, &lp, sizeof lp, 0, cudaMemcpyHostToDevice, st),
+            "wavefront launch block");
+  cudaCheck(cudaMemcpyToSymbolAsync(c_pool, &pool, sizeof pool, 0, cudaMemcpyHostToDevice, st),
+            "wavefront pool");
+  cudaCheck(cudaMemsetAsync(b.counts.ptr, 0, b.counts.bytes, st), "wavefront counts");
+  int launches = 0;
+  wfStart<<<b.gridStart, kRenderBlock, 0, st>>>();
+  cudaCheck(cudaGetLastError(), "wfStart");
+  launches++;
+  unsigned* counts = (unsigned*)b.counts.ptr;
+  int cur = 0;
+  for (int iter = 0;; iter++) {
+    int nxt = 1 - cur;
+    cudaCheck(cudaMemsetAsync(counts + nxt, 0, sizeof(unsigned), st), "wavefront counts");
+    cudaCheck(cudaMemsetAsync(counts + 2, 0, sizeof(unsigned), st), "wavefront counts");
+    wfTrace<<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
+    wfShadeA<<<b.gridShadeA, kRenderBlock, 0, st>>>(cur, nxt);
+    wfShadow<<<b.gridShadow, kRenderBlock, 0, st>>>();
+    wfShadeB<<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
+    cudaCheck(cudaGetLastError(), "wavefront stage");
+    launches += 4;
+    cur = nxt;
+    cudaCheck(cudaMemcpyAsync(b.hostCount, counts + cur, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                              st),
+              "wavefront count");
+    cudaCheck(cudaStreamSynchronize(st), "wavefront iteration");
+    if (*b.hostCount == 0) break;
+    if (iter > (1 << 24)) throw std::runtime_error("wavefront: no progress");
+  }
+  return launches;
+}
+
+}  // namespace sdb

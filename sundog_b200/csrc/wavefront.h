@@ -1,0 +1,48 @@
+// Wavefront path tracer (wavefront.cu): pool buffers and the host driver.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "render_session.h"
+#include "sd_types.h"
+
+namespace sdb {
+
+struct Path;
+struct Vertex;
+struct TraceHit;
+
+// Device view of the slot pool (one path per slot).
+struct WfPool {
+  Path* paths;
+  Vertex* verts;
+  TraceHit* hits;
+  float4* trs;             // shadow-ray transmittance of the slot's vertex
+  unsigned char* pending;  // 1: the slot's second half is due this iteration
+  int* lists[2];           // live slot lists, ping-pong between iterations
+  int* shadowList;
+  unsigned* counts;        // [0], [1]: list lengths; [2]: shadow-list length
+  int cap;
+};
+
+// Host-owned pool storage, grown on demand.
+struct WfBuffers {
+  DevBuf paths, verts, hits, trs, pending, list0, list1, shadow, counts;
+  unsigned* hostCount = nullptr;
+  int cap = 0;
+  int gridStart = 0, gridTrace = 0, gridShadeA = 0, gridShadow = 0, gridShadeB = 0;
+  WfBuffers() = default;
+  WfBuffers(const WfBuffers&) = delete;
+  WfBuffers& operator=(const WfBuffers&) = delete;
+  ~WfBuffers();
+  void ensure(int slots);
+};
+
+// Device bytes per pool slot.
+size_t wfSlotBytes();
+// Renders lp.numPaths camera paths (counters cleared by the caller) into
+// lp.sampleL; returns the number of kernels launched. Synchronises st once per
+// iteration to read the live-path count.
+int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st);
+
+}  // namespace sdb

@@ -291,7 +291,7 @@ class Scene(object):
             ok(rc, "light")
 
     # ---- rendering ----------------------------------------------------------------
-    def render_film(self, base_dir=".", aov=False, chunk_spp=0, **opts):
+    def render_film(self, base_dir=".", aov=False, chunk_spp=0, engine=0, **opts):
         """Render through sundog_render_ex; returns (film HxWx4, result, aovs)."""
         lib = abi.load()
         h = self.build(base_dir, lib)
@@ -305,7 +305,8 @@ class Scene(object):
             alb = np.zeros_like(film) if aov else None
             nrm = np.zeros_like(film) if aov else None
             ext = abi.RenderExt(film.ctypes.data, alb.ctypes.data if aov else None,
-                                nrm.ctypes.data if aov else None, chunk_spp, 1, 0, 0)
+                                nrm.ctypes.data if aov else None, chunk_spp, 1, 0, 0, 0,
+                                engine)
             res = abi.RenderResult()
             abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
                                            ctypes.byref(res)), "render", lib)
@@ -318,14 +319,14 @@ class Session(object):
     """A scene resident on the device (sundog_session_*)."""
 
     def __init__(self, scene, base_dir=".", aov=False, chunk_spp=0, guiding=0, sample_offset=0,
-                 frame_spp=0, **opts):
+                 frame_spp=0, engine=0, **opts):
         self.lib = abi.load()
         h = scene.build(base_dir, self.lib)
         try:
             o = abi.options(**opts)
             dummy = np.zeros(4, np.float32)
             ext = abi.RenderExt(None, dummy.ctypes.data if aov else None, None, chunk_spp, 1,
-                                guiding, sample_offset, frame_spp)
+                                guiding, sample_offset, frame_spp, engine)
             self.handle = self.lib.sundog_session_create(h, ctypes.byref(o), ctypes.byref(ext))
             if not self.handle:
                 raise abi.SundogError("session: " + abi.last_error(self.lib))

@@ -167,3 +167,33 @@ def test_sample_blocks_combine(lib, asset_dir):
     print("sample blocks: max rel diff %.2e" % err.max())
     assert err.max() <= 1e-4
     assert not np.array_equal(blocks[0], blocks[1])
+
+
+@pytest.mark.parametrize("name", ["cornell", "features", "instancing", "volumes"])
+def test_wavefront_matches_megakernel(lib, asset_dir, name):
+    """The wavefront engine (stage kernels over a slot pool) runs the same
+    per-path code in the same order with the same random draws as the
+    persistent megakernel: same samples, same ray count. Films agree to FP32
+    rounding (the stages are compiled in different kernels, so the compiler
+    may contract a few expressions differently)."""
+    if name == "cornell":
+        s, base = workloads.cornell(width=64, height=64, spp=16), "."
+    elif name == "features":
+        s, base = features_scene(), "."
+    elif name == "instancing":
+        s, base = workloads.instancing(asset_dir, width=96, height=54, spp=8), asset_dir
+    else:
+        s, base = workloads.volumes(asset_dir, width=80, height=45, spp=8), asset_dir
+    films, rays = [], []
+    for engine in (1, 2):
+        with sc.Session(s, base_dir=base, engine=engine) as ses:
+            res = ses.render()
+            films.append(ses.read()[..., :3].astype(np.float64))
+            rays.append(res.rays_traced)
+    same = np.mean(np.all(films[0] == films[1], axis=-1))
+    err = np.abs(films[0] - films[1]) / np.maximum(np.abs(films[0]), 1e-3)
+    print("%s: rays %d / %d, identical pixels %.4f, max rel diff %.2e" %
+          (name, rays[0], rays[1], same, err.max()))
+    assert abs(rays[0] - rays[1]) <= 1e-4 * rays[0]
+    assert np.quantile(err, 0.99) <= 1e-4
+    compare(name + " engines", films[1], films[0], frac_min=0.99, relmse_max=1e-4)

@@ -1,8 +1,8 @@
 """The render server (sundog_server_*): continuous batching of tile-passes
 from several jobs in one persistent launch.
 
-  * every job's film is bit-identical to a plain session render of the same
-    scene, size, spp and seed -- alone on the server and mixed with other
+  * every job's film is bit-identical to a session render of the same
+    scene, size, spp and seed with the persistent megakernel -- alone on the server and mixed with other
     scenes' jobs (ragged edge tiles, spp not a multiple of the pass size);
   * host-side failures end only the affected job: a missing asset (FAILED
     with the loader's message), a film larger than the device (FAILED, not
@@ -24,7 +24,8 @@ pytestmark = pytest.mark.gpu
 
 
 def session_film(s, base_dir, **opts):
-    with sc.Session(s, base_dir=base_dir, **opts) as ses:
+    # The server runs the persistent megakernel's path code (engine 1).
+    with sc.Session(s, base_dir=base_dir, engine=1, **opts) as ses:
         ses.render()
         return ses.read()
 
