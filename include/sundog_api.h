@@ -199,10 +199,11 @@ typedef struct {
                             of: the pixel strata follow it, so blocks rendered
                             apart (one per GPU) hold exactly the frame's
                             samples; <= 0 = this render's spp */
-  int32_t engine;        /* path-tracing kernels: 0 = automatic (wavefront for
-                            plain renders, megakernel for guided ones), 1 =
-                            persistent megakernel, 2 = wavefront (plain renders
-                            only). Both give the same samples. */
+  int32_t engine;        /* path-tracing kernels: 0 = automatic (wavefront,
+                            except guiding's training passes, which run in the
+                            persistent megakernel), 1 = persistent megakernel
+                            throughout, 2 = same as 0. Both engines give the
+                            same samples. */
 } sundog_render_ext;
 
 typedef struct {

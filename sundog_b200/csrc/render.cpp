@@ -573,11 +573,11 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
     cudaCheck(cudaMemsetAsync(lp.pathCounter, 0, sizeof(unsigned long long), st), "counter reset");
     cudaCheck(setLaunch(lp, st), "launch params");
     cudaCheck(cudaEventRecord(kev[0], st), "event");
-    const bool wavefront = mode == 0 && engine != 1;
+    const bool wavefront = (mode == 0 || mode == kGuideSample) && engine != 1;
     if (wavefront) {
       if (!wf) wf.reset(new WfBuffers());
       wf->ensure((int)std::min<unsigned long long>(lp.numPaths, kWavefrontSlots));
-      launches += wfRender(lp, *wf, st);
+      launches += wfRender(lp, *wf, st, mode);
     } else {
       cudaCheck(launchRender(st, grid, mode), "path kernel launch");
       launches += 1;

@@ -149,6 +149,9 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfShadow() 
   }
 }
 
+// GUIDE = kGuideSample: the BSDF sample by MIS with the learned guide
+// (sd_guide.cuh); the mixture table is in the launch block.
+template <int GUIDE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeB(int in, int out) {
   const SdLaunch& lp = c_wlp;
   const WfPool& pool = c_pool;
@@ -163,7 +166,7 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeB(in
       float4 t4 = pool.trs[slot];
       tr = v3(t4.x, t4.y, t4.z);
     }
-    if (finishVertex<0>(lp, p, v, tr)) {
+    if (finishVertex<GUIDE>(lp, p, v, tr)) {
       pool.paths[slot] = p;
       pool.lists[out][appendSlot(&pool.counts[out])] = slot;
     } else {
@@ -200,7 +203,7 @@ void WfBuffers::ensure(int slots) {
   gridTrace = gridFor(wfTrace);
   gridShadeA = gridFor(wfShadeA);
   gridShadow = gridFor(wfShadow);
-  gridShadeB = gridFor(wfShadeB);
+  gridShadeB = gridFor(wfShadeB<0>);
   gridStart = gridFor(wfStart);
 }
 
@@ -214,7 +217,9 @@ size_t wfSlotBytes() {
 
 // Renders the launch block's paths (lp.numPaths ids, counters already
 // cleared) into lp.sampleL through the stages. Returns the kernels launched.
-int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st) {
+int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
+  if (guide != 0 && guide != kGuideSample)
+    throw std::runtime_error("wavefront: training passes run in the persistent kernel");
   WfPool pool;
   pool.paths = (Path*)b.paths.ptr;
   pool.verts = (Vertex*)b.verts.ptr;
@@ -244,7 +249,10 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st) {
     wfTrace<<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
     wfShadeA<<<b.gridShadeA, kRenderBlock, 0, st>>>(cur, nxt);
     wfShadow<<<b.gridShadow, kRenderBlock, 0, st>>>();
-    wfShadeB<<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
+    if (guide == kGuideSample)
+      wfShadeB<kGuideSample><<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
+    else
+      wfShadeB<0><<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
     cudaCheck(cudaGetLastError(), "wavefront stage");
     launches += 4;
     cur = nxt;

@@ -42,7 +42,9 @@ struct WfBuffers {
 size_t wfSlotBytes();
 // Renders lp.numPaths camera paths (counters cleared by the caller) into
 // lp.sampleL; returns the number of kernels launched. Synchronises st once per
-// iteration to read the live-path count.
-int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st);
+// iteration to read the live-path count. guide: 0, or kGuideSample to draw
+// directions by MIS with the learned guide of lp (training passes, which keep
+// per-path records, run in the persistent kernel).
+int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide = 0);
 
 }  // namespace sdb
