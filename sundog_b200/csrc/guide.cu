@@ -3,8 +3,8 @@
 //
 // Network (guide_net.h): 48 inputs -> 3 x 64 ReLU -> 48 outputs describing an
 // 8-lobe von Mises-Fisher mixture over incident directions. Weights are BF16,
-// every product accumulates in FP32 on the tensor cores
-// (mma.m16n8k16.bf16, FP32 accumulators).
+// every product accumulates in FP32 on the tensor cores (tcgen05.mma kind::f16
+// for inference, mma.m16n8k16.bf16 in the fused training step).
 //
 // guideTrainKernel: one fused forward + backward pass over a batch of
 //   training records. A warp owns 16 records; the activations of all three
@@ -16,8 +16,13 @@
 //   gradients dW = dZ^T H reduce over the CTA's 128 records with MMAs on
 //   transposed copies in shared memory and are accumulated in shared memory
 //   across the CTA's tiles, then added to the global gradient once per CTA.
-// guideForwardKernel: the forward pass alone, for the cache bake (one row
-//   per grid cell and normal direction) and for the raw-output check.
+// guideForwardTc: the forward pass alone on tcgen05 tensor cores (TMEM
+//   accumulators, one elected thread issuing the MMAs), for the mixture-table
+//   bake (one row per grid cell and normal direction) and the raw-output
+//   check. The fused training kernel keeps warp-level MMAs: its backward
+//   pass reduces weight gradients over records with transposed operands that
+//   live in registers between layers, and at 64-wide layers its time goes to
+//   barriers and the per-record loss head, not to the MMA rate.
 // guideAdamKernel: Adam on the FP32 master parameters; refreshes the BF16
 //   weight copy.
 //
@@ -59,8 +64,8 @@ constexpr int kST = kTileRows + 8;      //   the fragment loads below
 constexpr int kOutStride = 49;
 constexpr float kWeightClamp = 100.0f;
 
-// Shared-memory carve-up (bytes). The forward-only kernels use the part up
-// to kSmemForward.
+// Shared-memory carve-up of the training kernel (bytes): weights, biases and
+// output tiles first, then the backward pass's transposes and accumulators.
 constexpr int oSW0 = 0;
 constexpr int oSW1 = oSW0 + kNetHid * kS48 * 2;
 constexpr int oSW2 = oSW1 + kNetHid * kS64 * 2;
@@ -524,60 +529,262 @@ struct ForwardArgs {
 };
 
 // Bake mode (queries == nullptr): row = grid cell x normal direction, with
-// the cell centre as position; writes the cache entries sd_guide.cuh reads.
-__global__ void __launch_bounds__(kThreads) guideForwardKernel(ForwardArgs a) {
-  extern __shared__ __align__(16) unsigned char sm[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2;
-  loadNet(sm, a.wb, a.params, false);
+// the cell centre as position, and the kernel writes the cache entries
+// sd_guide.cuh reads; otherwise raw outputs for the queries.
+// ---- forward pass on tcgen05 (5th-generation tensor cores, TMEM accumulators) --
+//
+// One CTA of 128 threads runs 128 rows through the network, one row per
+// thread: thread t builds row t's input features and, after each layer, reads
+// row t of the accumulator from tensor memory (TMEM lane t). A layer is K/16
+// tcgen05.mma steps of M=128 x N x K=16 issued by one thread, BF16 operands
+// from shared memory, FP32 accumulators in TMEM, completion signalled through
+// an mbarrier. Operands use the canonical K-major layout without swizzle:
+// core matrices of 8 rows x 16 bytes, the two 8-element K halves of a step
+// 128 bytes apart (leading offset), 8-row groups K*16 bytes apart (stride
+// offset). The activations between layers go TMEM -> registers (bias, ReLU,
+// BF16) -> shared memory, never to global memory.
+namespace tc {
+
+constexpr int kRows = 128;
+constexpr int kCtaThreads = 128;
+constexpr int oW0 = 0;                               // 64 x 48
+constexpr int oW1 = oW0 + kNetHid * kNetIn * 2;      // 64 x 64
+constexpr int oW2 = oW1 + kNetHid * kNetHid * 2;     // 64 x 64
+constexpr int oW3 = oW2 + kNetHid * kNetHid * 2;     // 48 x 64
+constexpr int oA = oW3 + kNetOut * kNetHid * 2;      // 128 x 64 activations
+constexpr int oBias = oA + kRows * kNetHid * 2;
+constexpr int oBar = oBias + (kNetParams - kNetWeights) * 4;
+constexpr int oTmem = oBar + 8;
+constexpr int kSmem = oTmem + 8;
+constexpr uint32_t kTmemCols = 64;                   // N <= 64 FP32 accumulators
+constexpr unsigned kWaitLimit = 1u << 24;            // mbarrier polls before giving up
+static_assert(oA % 128 == 0 && oBar % 8 == 0, "tcgen05 shared-memory layout");
+
+// Byte offset of element (r, k) of a K-major matrix with K columns.
+__device__ __forceinline__ uint32_t coreOff(int r, int k, int K) {
+  return (uint32_t)((r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// Shared-memory matrix descriptor: start address, leading byte offset 128,
+// stride byte offset K*16, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t smemDesc(uint32_t saddr, int K) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
+         ((uint64_t)((((uint32_t)K * 16u) >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N and M encoded as N/8 and M/16.
+__device__ __forceinline__ uint32_t instrDesc(int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(kRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma(uint32_t dTmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                    uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+      :
+      : "r"(dTmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :
+               : "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool tryWait(uint32_t bar, uint32_t phase) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(done)
+      : "r"(bar), "r"(phase)
+      : "memory");
+  return done != 0;
+}
+
+// 16 FP32 accumulator columns [col, col+16) of this thread's TMEM lane.
+__device__ __forceinline__ void ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
+}
+
+}  // namespace tc
+
+__device__ int g_tcTimeout;  // set when an mbarrier wait hit its limit
+
+__global__ void __launch_bounds__(tc::kCtaThreads, 4) guideForwardTc(ForwardArgs a) {
+  using namespace tc;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int t = threadIdx.x, warp = t >> 5;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+  const uint32_t bar = sbase + oBar;
+  float* sB = (float*)(sm + oBias);
+
+  // Weights in the canonical layout, biases, barrier, TMEM.
+  for (int i = t; i < kNetWeights; i += kCtaThreads) {
+    unsigned short w = reinterpret_cast<const unsigned short*>(a.wb)[i];
+    uint32_t off;
+    if (i < kOffW1) off = oW0 + coreOff(i / kNetIn, i % kNetIn, kNetIn);
+    else if (i < kOffW2) off = oW1 + coreOff((i - kOffW1) / kNetHid, (i - kOffW1) % kNetHid, kNetHid);
+    else if (i < kOffW3) off = oW2 + coreOff((i - kOffW2) / kNetHid, (i - kOffW2) % kNetHid, kNetHid);
+    else off = oW3 + coreOff((i - kOffW3) / kNetHid, (i - kOffW3) % kNetHid, kNetHid);
+    *reinterpret_cast<unsigned short*>(sm + off) = w;
+  }
+  for (int i = t; i < kNetParams - kNetWeights; i += kCtaThreads) sB[i] = a.params[kNetWeights + i];
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     sbase + oTmem),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  float* sOut = (float*)(sm + oSOut) + warp * 16 * kOutStride;
-  const int tiles = (a.rows + kTileRows - 1) / kTileRows;
-  auto query = [&](int row, float3& p, float3& n) {
-    row = min(row, a.rows - 1);
-    if (a.queries) {
-      const float* q = a.queries + 6 * (size_t)row;
-      p = v3(q[0], q[1], q[2]);
-      n = v3(q[3], q[4], q[5]);
-      return;
-    }
-    int bin = row % kGuideNormals, cell = row / kGuideNormals;
-    int iz = cell % kGuideGrid, iy = (cell / kGuideGrid) % kGuideGrid, ix = cell / (kGuideGrid * kGuideGrid);
-    const float inv = 1.0f / kGuideGrid;
-    p = v3((ix + 0.5f) * inv, (iy + 0.5f) * inv, (iz + 0.5f) * inv);
-    float sgn = (bin & 1) ? -1.0f : 1.0f;
-    n = v3(bin >> 1 == 0 ? sgn : 0.0f, bin >> 1 == 1 ? sgn : 0.0f, bin >> 1 == 2 ? sgn : 0.0f);
-  };
-  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const int rowBase = tile * kTileRows + warp * 16;
-    Acts act;
-    float3 p0, n0, p1, n1;
-    query(rowBase + g, p0, n0);
-    query(rowBase + g + 8, p1, n1);
-    inputFrags(p0, n0, p1, n1, act.x);
-    forwardWarp(sm, act, sOut);
-    __syncwarp();
-    int row = rowBase + lane;
-    if (lane < 16 && row < a.rows) {
-      float o[kNetLobeOut];
-      for (int j = 0; j < kNetLobeOut; j++) o[j] = sOut[lane * kOutStride + j];
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + oTmem);
+  const uint32_t myLane = tmem + ((uint32_t)(warp * 32) << 16);
+
+  const int layerK[4] = {kNetIn, kNetHid, kNetHid, kNetHid};
+  const int layerN[4] = {kNetHid, kNetHid, kNetHid, kNetOut};
+  const int layerW[4] = {oW0, oW1, oW2, oW3};
+  const int layerB[4] = {kOffB0 - kNetWeights, kOffB1 - kNetWeights, kOffB2 - kNetWeights,
+                         kOffB3 - kNetWeights};
+  uint32_t phase = 0;
+  bool failed = false;
+  const int tiles = (a.rows + kRows - 1) / kRows;
+  for (int tile = blockIdx.x; tile < tiles && !failed; tile += gridDim.x) {
+    const int row = tile * kRows + t;
+    // Input features of this thread's row (same definition as featurePair).
+    {
+      int r = min(row, a.rows - 1);
+      float3 p, n;
       if (a.queries) {
-        for (int j = 0; j < kNetLobeOut; j++) a.outputs[(size_t)row * kNetLobeOut + j] = o[j];
+        const float* q = a.queries + 6 * (size_t)r;
+        p = v3(q[0], q[1], q[2]);
+        n = v3(q[3], q[4], q[5]);
+      } else {
+        int bin = r % kGuideNormals, cell = r / kGuideNormals;
+        int iz = cell % kGuideGrid, iy = (cell / kGuideGrid) % kGuideGrid,
+            ix = cell / (kGuideGrid * kGuideGrid);
+        const float inv = 1.0f / kGuideGrid;
+        p = v3((ix + 0.5f) * inv, (iy + 0.5f) * inv, (iz + 0.5f) * inv);
+        float sgn = (bin & 1) ? -1.0f : 1.0f;
+        n = v3(bin >> 1 == 0 ? sgn : 0.0f, bin >> 1 == 1 ? sgn : 0.0f, bin >> 1 == 2 ? sgn : 0.0f);
+      }
+      for (int col = 0; col < kNetIn; col += 2) {
+        uint32_t pr = featurePair(p, n, col);
+        *reinterpret_cast<uint32_t*>(sm + oA + coreOff(t, col, kNetIn)) = pr;
+      }
+    }
+    float out[kNetOut];
+    for (int l = 0; l < 4 && !failed; l++) {
+      const int K = layerK[l], N = layerN[l];
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (t == 0) {
+        const uint32_t idesc = instrDesc(N);
+        for (int kk = 0; kk < K / 16; kk++)
+          mma(tmem, smemDesc(sbase + oA + kk * 256, K), smemDesc(sbase + layerW[l] + kk * 256, K),
+              idesc, kk > 0 ? 1u : 0u);
+        commit(bar);
+      }
+      unsigned polls = 0;
+      bool timedOut = false;
+      while (!tryWait(bar, phase)) {
+        if (++polls >= kWaitLimit) {
+          timedOut = true;
+          break;
+        }
+      }
+      phase ^= 1u;
+      // One decision for the whole block, so no thread is left at a barrier.
+      failed = __syncthreads_or(timedOut) != 0;
+      if (failed) {
+        if (t == 0) atomicExch(&g_tcTimeout, 1);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      float acc[64];
+      for (int c = 0; c < N; c += 16) {
+        float v[16];
+        tc::ld16(myLane + (uint32_t)c, v);
+#pragma unroll
+        for (int j = 0; j < 16; j++) acc[c + j] = v[j];
+      }
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const float* bias = sB + layerB[l];
+      if (l < 3) {
+        // Next layer's operand: this row, 64 BF16 values after bias + ReLU.
+        for (int c = 0; c < kNetHid; c += 2) {
+          uint32_t pr = pack2(fmaxf(acc[c] + bias[c], 0.0f), fmaxf(acc[c + 1] + bias[c + 1], 0.0f));
+          *reinterpret_cast<uint32_t*>(sm + oA + coreOff(t, c, kNetHid)) = pr;
+        }
+      } else {
+        for (int c = 0; c < kNetOut; c++) out[c] = acc[c] + bias[c];
+      }
+    }
+    if (failed) break;
+    if (row < a.rows) {
+      if (a.queries) {
+        for (int j = 0; j < kNetLobeOut; j++) a.outputs[(size_t)row * kNetLobeOut + j] = out[j];
       } else {
         Lobe L[kGuideLobes];
-        decodeLobes(o, L);
-        float acc = 0.0f;
+        decodeLobes(out, L);
+        float accw = 0.0f;
         for (int k = 0; k < kGuideLobes; k++) {
           float kap = L[k].kappa;
           float3 km = L[k].mu * kap;
           a.lobes[(size_t)row * kGuideLobes + k] =
               make_float4(km.x, km.y, km.z, L[k].logw + vmfLogNorm(kap) - kap);
-          acc += expf(L[k].logw);
-          a.cdf[(size_t)row * kGuideLobes + k] = acc;
+          accw += expf(L[k].logw);
+          a.cdf[(size_t)row * kGuideLobes + k] = accw;
         }
       }
     }
-    __syncwarp();
   }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
+}
+
+int smCount();
+
+// Runs guideForwardTc over f.rows rows; throws if a completion wait timed out.
+void runForwardTc(const ForwardArgs& f, cudaStream_t st) {
+  int zero = 0;
+  cudaCheck(cudaMemcpyToSymbolAsync(g_tcTimeout, &zero, sizeof zero, 0, cudaMemcpyHostToDevice, st),
+            "tcgen05 flag");
+  int tiles = (f.rows + tc::kRows - 1) / tc::kRows;
+  guideForwardTc<<<std::min(tiles, smCount() * 4), tc::kCtaThreads, tc::kSmem, st>>>(f);
+  cudaCheck(cudaGetLastError(), "guide forward (tcgen05)");
+  int flag = 0;
+  cudaCheck(cudaMemcpyFromSymbolAsync(&flag, g_tcTimeout, sizeof flag, 0, cudaMemcpyDeviceToHost, st),
+            "tcgen05 flag");
+  cudaCheck(cudaStreamSynchronize(st), "guide forward (tcgen05)");
+  if (flag) throw std::runtime_error("guide forward: tensor-core completion wait timed out");
 }
 
 __global__ void guideAdamKernel(float* P, float* G, float* M, float* V, bf16* wb, float lr,
@@ -628,9 +835,7 @@ void enableSmem() {
   cudaCheck(cudaFuncSetAttribute(guideTrainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kSmemTrain),
             "guide train smem");
-  cudaCheck(cudaFuncSetAttribute(guideForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kSmemForward),
-            "guide forward smem");
+
   if (dev < 64) done |= 1ull << dev;
 }
 
@@ -859,9 +1064,7 @@ void GuideState::bake(cudaStream_t st) {
   f.outputs = nullptr;
   f.lobes = (float4*)lobes.ptr;
   f.cdf = (float*)cdf.ptr;
-  int tiles = (kGuideCells + kTileRows - 1) / kTileRows;
-  guideForwardKernel<<<std::min(tiles, smCount() * 4), kThreads, kSmemForward, st>>>(f);
-  cudaCheck(cudaGetLastError(), "guide bake");
+  runForwardTc(f, st);
   cudaCheck(cudaEventRecord(b1, st), "event");
   cudaCheck(cudaEventSynchronize(b1), "guide bake");
   float ms = 0.0f;
@@ -954,9 +1157,7 @@ extern "C" int sundog_guide_outputs(const float* params, const float* queries, i
   f.outputs = (float*)o.ptr;
   f.lobes = nullptr;
   f.cdf = nullptr;
-  int tiles = (n + kTileRows - 1) / kTileRows;
-  guideForwardKernel<<<std::min(tiles, smCount() * 4), kThreads, kSmemForward>>>(f);
-  cudaCheck(cudaGetLastError(), "guide forward");
+  runForwardTc(f, nullptr);
   cudaCheck(cudaMemcpy(outputs, o.ptr, o.bytes, cudaMemcpyDeviceToHost), "outputs");
   return SUNDOG_OK;
   SDB_CATCH(SUNDOG_ERROR)
