@@ -395,7 +395,13 @@ class Server {
   }
 
   // Next tile-pass of job j not yet in this batch; false when none is left.
-  bool nextTilePass(ServeJob& j, std::vector<char>& used, ServeItem& it) {
+  int tileNpad(const ServeJob& j, int t) const {
+    int x0 = (t % j.tilesX) * cfg.tile, y0 = (t / j.tilesX) * cfg.tile;
+    int w = std::min(cfg.tile, j.width - x0), h = std::min(cfg.tile, j.height - y0);
+    return ((w + 7) / 8) * ((h + 7) / 8) * 64;
+  }
+
+  bool nextTilePass(ServeJob& j, std::vector<char>& used, int chunk, ServeItem& it) {
     int nt = (int)j.tileNext.size();
     for (int k = 0; k < nt; k++) {
       int t = (j.cursor + k) % nt;
@@ -411,7 +417,7 @@ class Server {
       it.bw = (it.w + 7) / 8;
       it.npad = it.bw * ((it.h + 7) / 8) * 64;
       it.sampleBegin = j.tileNext[t];
-      it.sampleCount = std::min(cfg.pass_spp, j.spp - j.tileNext[t]);
+      it.sampleCount = std::min(chunk, j.spp - j.tileNext[t]);
       it.pad0 = t;  // tile index, for the host's bookkeeping
       return true;
     }
@@ -429,11 +435,24 @@ class Server {
     });
     std::vector<std::vector<char>> used(act.size());
     for (size_t i = 0; i < act.size(); i++) used[i].assign(act[i]->tileNext.size(), 0);
+    // Samples per tile-pass: pass_spp, or more when every remaining tile at
+    // pass_spp would not fill the path budget (few or small jobs left), so
+    // the launch stays full. The batch stays within the budget: each item is
+    // at most `factor` times its tile's share of `demand`.
+    uint64_t demand = 0;
+    for (auto& j : act)
+      for (int t = 0; t < (int)j->tileNext.size(); t++)
+        if (j->tileNext[t] < j->spp)
+          demand += (uint64_t)tileNpad(*j, t) * std::min(cfg.pass_spp, j->spp - j->tileNext[t]);
+    int chunk = cfg.pass_spp;
+    if (demand > 0 && demand < cfg.iteration_paths)
+      chunk = (int)std::min<uint64_t>((uint64_t)cfg.pass_spp * (cfg.iteration_paths / demand), 4096);
+    const uint64_t itemMax = (uint64_t)((cfg.tile + 7) / 8) * ((cfg.tile + 7) / 8) * 64 * chunk;
     int n = 0;
     uint64_t total = 0;
     auto add = [&](size_t i) {
       ServeItem it;
-      if (n >= maxItems || !nextTilePass(*act[i], used[i], it)) return false;
+      if (n >= maxItems || !nextTilePass(*act[i], used[i], chunk, it)) return false;
       it.pathBegin = total;
       total += (uint64_t)it.npad * it.sampleCount;
       hItems[n++] = it;
@@ -441,7 +460,7 @@ class Server {
     };
     for (size_t i = 0; i < act.size(); i++) add(i);  // one tile-pass each
     for (size_t i = 0; i < act.size(); i++)
-      while (total + maxItemPaths <= cfg.iteration_paths && add(i)) {
+      while (total + itemMax <= cfg.iteration_paths && add(i)) {
       }
     if (n == 0) return;
     cudaCheck(cudaMemcpyAsync(dItems.ptr, hItems, (size_t)n * sizeof(ServeItem),
