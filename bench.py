@@ -146,12 +146,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_path():
-    """DRAM bytes (read + write) per camera path of the path kernel, from the
-    committed ncu summary of a smaller launch of the same workload (traffic
-    is per-path work: the per-sample radiance write and evicted stack
-    lines), so a launch's traffic is this times its paths."""
-    p = os.path.join(ROOT, "profiles", "pt_persistent_instancing.md")
+def ncu_traffic_per_path(engine=0):
+    """DRAM bytes (read + write) per camera path of the path-tracing kernels,
+    from the committed ncu summary of a smaller render of the same workload
+    (traffic is per-path work: path state between stages, per-sample
+    radiance writes, stack lines), so a chunk's traffic is this times its
+    paths. engine 1 = the persistent megakernel, else the wavefront engine."""
+    name = "pt_persistent_instancing.md" if engine == 1 else "wf_trace_instancing.md"
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.isfile(p):
         return None
     with open(p) as f:
@@ -351,13 +353,14 @@ def run_ours(args):
         counts = abi.TraceCounts()
         abi.check(lib.sundog_session_trace_counts(ses.handle, ctypes.byref(counts)), "counts", lib)
         bpr = bytes_per_ray(counts)
-        launches_per_step = launches / args.steps
-        kernel_launches = max(1, int(round(launches_per_step / 2)))  # persistent launches
+        # Roofline unit: one chunk of samples (one persistent launch, or one
+        # wavefront pass over the chunk's paths), timed by the session's events.
+        kernel_launches = max(1, -(-args.spp // max(st.chunk_spp, 1)))  # chunks per step
         mean_launch_ms = kernel_ms / (args.steps * kernel_launches)
         rays_per_launch = rays / (args.steps * kernel_launches)
         achieved = bpr * rays_per_launch / (mean_launch_ms / 1000.0) / 1e9
         peak, peak_kind = measured_peaks()
-        per_path = ncu_traffic_per_path()
+        per_path = ncu_traffic_per_path(args.engine)
         paths_per_launch = args.width * args.height * args.spp / kernel_launches
         traffic = per_path * paths_per_launch if per_path is not None else None
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -372,9 +375,9 @@ def run_ours(args):
                              "path_loop_lanes_per_iter": counts.loop_lanes / max(counts.loop_iters, 1),
                              "traversal_iters_per_ray": 32.0 * counts.trav_iters / max(counts.rays, 1)},
                     "note": "algorithmic bytes on a binary BVH (32 B/box, 36 B/tri, 48 B/"
-                            "quadric, 64 B/instance) per path-kernel launch over its CUDA-event "
-                            "duration; the BVH (<4 MB) and env tables are L2-resident, so HBM "
-                            "is a loose bound"}
+                            "quadric, 64 B/instance) per chunk of samples (one persistent launch "
+                            "or one wavefront pass) over its CUDA-event duration; the BVH (<4 MB) "
+                            "and env tables are cache-resident, so HBM is a loose bound"}
         cpu = None
         if not args.no_cpu_baseline:
             cpu, _, _ = oracle_sample(scene, base, args, args.cpu_seconds, os.cpu_count() or 1)

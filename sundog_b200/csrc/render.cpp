@@ -151,7 +151,7 @@ static int strataFor(int spp) {  // device/programs.cu:317-319
 }
 
 RenderSession::~RenderSession() {
-  wf.reset();
+  wfRelease(std::move(wf));
   if (stream) cudaStreamDestroy(stream);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
@@ -575,7 +575,7 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
     cudaCheck(cudaEventRecord(kev[0], st), "event");
     const bool wavefront = (mode == 0 || mode == kGuideSample) && engine != 1;
     if (wavefront) {
-      if (!wf) wf.reset(new WfBuffers());
+      if (!wf) wf = wfAcquire();
       wf->ensure((int)std::min<unsigned long long>(lp.numPaths, kWavefrontSlots));
       launches += wfRender(lp, *wf, st, mode);
     } else {

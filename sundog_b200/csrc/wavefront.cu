@@ -23,6 +23,8 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <memory>
+#include <mutex>
 #include <stdexcept>
 
 #include "pt_path.cuh"
@@ -209,6 +211,28 @@ void WfBuffers::ensure(int slots) {
 
 WfBuffers::~WfBuffers() {
   if (hostCount) cudaFreeHost(hostCount);
+}
+
+// One idle pool per device, kept between sessions: a one-shot render
+// (sundog_render, sundog_render_ex) would otherwise allocate and free 1.3 GB
+// of slots per call.
+static std::mutex g_poolMu;
+static std::unique_ptr<WfBuffers> g_idle[64];
+
+std::unique_ptr<WfBuffers> wfAcquire() {
+  int dev = 0;
+  cudaCheck(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(g_poolMu);
+  if (dev >= 0 && dev < 64 && g_idle[dev]) return std::move(g_idle[dev]);
+  return std::unique_ptr<WfBuffers>(new WfBuffers());
+}
+
+void wfRelease(std::unique_ptr<WfBuffers> b) {
+  if (!b) return;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(g_poolMu);
+  if (!g_idle[dev] || g_idle[dev]->cap < b->cap) g_idle[dev] = std::move(b);
 }
 
 size_t wfSlotBytes() {

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
+
 #include "render_session.h"
 #include "sd_types.h"
 
@@ -40,6 +42,10 @@ struct WfBuffers {
 
 // Device bytes per pool slot.
 size_t wfSlotBytes();
+// A pool for the current device: the idle one kept from an earlier session,
+// or a new empty one. wfRelease keeps a finished session's pool for reuse.
+std::unique_ptr<WfBuffers> wfAcquire();
+void wfRelease(std::unique_ptr<WfBuffers> b);
 // Renders lp.numPaths camera paths (counters cleared by the caller) into
 // lp.sampleL; returns the number of kernels launched. Synchronises st once per
 // iteration to read the live-path count. guide: 0, or kGuideSample to draw
