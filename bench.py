@@ -15,9 +15,11 @@ flushed (256 MiB write) between steps; `e2e` is the same metric through
 sundog_render_ex with host buffers (asset load, CDF + BVH build, uploads,
 render, film download all inside the timed call).
 
-Multi-GPU (torchrun): one process per GPU; each rank renders its own 64-sample
-block of the same frame (samples [64 r, 64 r + 64)), no data-path
-collective; scaling "weak"; time = max over ranks.
+Multi-GPU (torchrun): one process per GPU; with N ranks the frame takes
+64 N spp and rank r renders its 64x64 film tiles t with t % N == r (every
+rank about the one-GPU frame's paths: scaling "weak"); no data-path
+collective, time = max over ranks; one all-gather of the disjoint films
+after the timed steps assembles the frame (film_gather_ms).
 
 --impl reference: the CPU oracle (oracle/, a restatement of the reference's
 render path; the reference itself needs OptiX and cannot run here) on the
@@ -66,6 +68,9 @@ def parse_args():
     ap.add_argument("--guide-spp", type=int, default=256)
     ap.add_argument("--guide-ref-spp", type=int, default=16384)
     ap.add_argument("--guide-seeds", type=int, default=4)
+    ap.add_argument("--guide-scene", default="volumes", choices=["volumes", "instancing"],
+                    help="scene of the guiding line: flame / water / glass (volumes) or "
+                         "1024 instances under the sun-and-sky env map (instancing)")
     ap.add_argument("--serving", action="store_true",
                     help="render-server line (Poisson jobs, p50/p99 latency) instead of Mrays/s")
     ap.add_argument("--serve-jobs", type=int, default=60)
@@ -231,12 +236,13 @@ def run_reference(args):
 
 # ---- ranks ---------------------------------------------------------------------------------
 
-def sample_block(rank, spp):
-    """Samples [first, first + count) of the frame that `rank` renders: each
-    rank a disjoint block of spp samples (weak scaling, no data-path
-    collective; the blocks' films are independent estimates of one image,
-    averaged with equal weights)."""
-    return rank * spp, spp
+def shard_plan(rank, world, spp):
+    """Rank's part of the job: the 64x64 film tiles t with t % world == rank
+    of one frame of spp x world samples (sundog_render_ext shard_count /
+    shard_index). Weak scaling: every rank traces about the one-GPU frame's
+    paths. No data-path collective; the disjoint films are gathered once after
+    the timed steps, into the frame a single GPU would render bit for bit."""
+    return {"shard_count": world if world > 1 else 0, "shard_index": rank, "spp": spp * world}
 
 
 def reduce_max_sum(dist, device, t_max, *sums):
@@ -274,9 +280,10 @@ def run_ours(args):
 
     scene = make_scene(args)
     base = asset_dir()
-    offset, _ = sample_block(rank, args.spp)
-    ses = sc.Session(scene, base_dir=base, sample_offset=offset, frame_spp=args.spp * world,
-                     engine=args.engine)
+    plan = shard_plan(rank, world, args.spp)
+    fspp = plan["spp"]
+    ses = sc.Session(scene, base_dir=base, engine=args.engine, shard_count=plan["shard_count"],
+                     shard_index=rank, spp=fspp)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -288,7 +295,7 @@ def run_ours(args):
         dist.barrier()
     torch.cuda.synchronize()
     clocks.start()
-    step_ms, rays, launches, kernel_ms = [], 0, 0, 0.0
+    step_ms, rays, paths, launches, kernel_ms = [], 0, 0, 0, 0.0
     t_wall = time.perf_counter()
     for _ in range(args.steps):
         flush.fill_(1)  # evict L2 between timed steps
@@ -300,25 +307,42 @@ def run_ours(args):
         e1.synchronize()
         step_ms.append(e0.elapsed_time(e1))
         rays += res.rays_traced
+        paths += res.paths
         launches += res.kernel_launches
         kernel_ms += res.kernel_ms
     torch.cuda.synchronize()
     wall = time.perf_counter() - t_wall
     clk = clocks.stop()
-    total_ms, rays_all = reduce_max_sum(dist, "cuda", float(sum(step_ms)), rays)
+    total_ms, rays_all, paths_all = reduce_max_sum(dist, "cuda", float(sum(step_ms)), rays, paths)
     value = rays_all / (total_ms / 1000.0) / 1e6
 
+    # The frame on every rank: one all-gather of the disjoint tile films
+    # (after the timed steps; not part of `value`).
+    gather_ms = None
+    if dist:
+        from sundog_b200 import shard
+        film = shard.session_film(ses)
+        torch.cuda.synchronize()
+        dist.barrier()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        shard.gather(film, world)
+        g1.record(stream)
+        g1.synchronize()
+        gather_ms, = reduce_max_sum(dist, "cuda", g0.elapsed_time(g1))
+
     # End to end through the public API with host buffers, every rank its
-    # own sample block (asset load, CDF + BVH build, upload, render, film
+    # own tile shard (asset load, CDF + BVH build, upload, render, film
     # download inside the timed call); whole job = slowest rank, summed rays.
     e2e = None
     if not args.no_e2e:
         h = scene.build(base, lib)
         try:
             film = np.zeros((args.height, args.width, 4), np.float32)
-            o = abi.options(quiet=True)
-            ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, offset, args.spp * world,
-                                args.engine)
+            o = abi.options(quiet=True, spp=fspp)
+            ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, 0, 0, args.engine,
+                                plan["shard_count"], rank)
             rr = abi.RenderResult()
             abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
                                            ctypes.byref(rr)), "render_ex", lib)  # warm
@@ -344,6 +368,8 @@ def run_ours(args):
                "h2d_bytes_per_step": int(hb / e_steps),
                "d2h_bytes_per_step": int(db / e_steps),
                "ms_per_step": 1000.0 * et / e_steps,
+               "last_call_ms": {"load": rr.load_ms, "build": rr.build_ms,
+                                "render": rr.render_ms, "total": rr.total_ms},
                "path": "sundog_render_ex per rank: OBJ/HDR load, CDF + BVH build, upload, "
                        "render, film download; slowest rank"}
 
@@ -355,13 +381,13 @@ def run_ours(args):
         bpr = bytes_per_ray(counts)
         # Roofline unit: one chunk of samples (one persistent launch, or one
         # wavefront pass over the chunk's paths), timed by the session's events.
-        kernel_launches = max(1, -(-args.spp // max(st.chunk_spp, 1)))  # chunks per step
+        kernel_launches = max(1, -(-fspp // max(st.chunk_spp, 1)))  # chunks per step
         mean_launch_ms = kernel_ms / (args.steps * kernel_launches)
         rays_per_launch = rays / (args.steps * kernel_launches)
         achieved = bpr * rays_per_launch / (mean_launch_ms / 1000.0) / 1e9
         peak, peak_kind = measured_peaks()
         per_path = ncu_traffic_per_path(args.engine)
-        paths_per_launch = args.width * args.height * args.spp / kernel_launches
+        paths_per_launch = paths / args.steps / kernel_launches
         traffic = per_path * paths_per_launch if per_path is not None else None
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "traffic": traffic,
@@ -386,15 +412,17 @@ def run_ours(args):
                 "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "width": args.width, "height": args.height,
-                           "spp": args.spp, "paths_per_step": args.width * args.height * args.spp,
+                           "spp": args.spp, "paths_per_step": int(paths_all / args.steps),
                            "l2": "flushed between steps (256 MiB write); BVH + env tables "
                                  "re-fetched each step",
-                           "parallelism": "dp%d (rank r renders samples [spp r, spp (r+1)))" % world,
+                           "parallelism": ("dp%d: rank r renders the 64x64 tiles t with t %% %d == r "
+                                           "of one %d-spp frame" % (world, world, fspp))
+                                          if world > 1 else "dp1 (whole frame)",
                            "grid": st.grid, "block": st.block, "chunk_spp": st.chunk_spp,
                            "engine": ["automatic (wavefront)", "megakernel",
                                       "wavefront"][args.engine]},
-                "samples_per_sec": args.width * args.height * args.spp * world /
-                                   (total_ms / 1000.0 / args.steps) if total_ms else None,
+                "samples_per_sec": paths_all / (total_ms / 1000.0) if total_ms else None,
+                "film_gather_ms": gather_ms,
                 "wall_s": wall,
                 "gpu_launches": launches,
                 "roofline": roofline,
@@ -420,29 +448,38 @@ def _relmse(img, ref):
 
 
 def run_guiding(args):
-    """Learned guiding on the flame / water / glass scene at 640x360, against
-    a 16384-spp plain render of the same scene. The scene's error is
-    dominated by rare high-energy paths (glossy panels lit by the flame's
-    point lights), so one render's relMSE is too noisy to rank two methods:
-    each method renders the frame with K seeds, and its error at a given
-    time is its mean relMSE over the seeds scaled by (its render time /
-    that time) -- MSE falls as 1 / samples for an unbiased estimator. The
-    guided time includes online training on the first 32 spp. `value` =
-    equal-time relMSE ratio plain / guided. Prints one JSON line."""
+    """Learned guiding at 640x360 against a 16384-spp plain render of the
+    same scene: the flame / water / glass scene (volumes) or the 1024-instance
+    field under the sun-and-sky env map (instancing). Rare high-energy paths
+    make one render's relMSE too noisy to rank two methods: each method
+    renders the frame with K seeds, and its error at a given time is its mean
+    relMSE over the seeds scaled by (its render time / that time) -- MSE
+    falls as 1 / samples for an unbiased estimator. The guided time includes
+    online training on the first 32 spp. `value` = equal-time relMSE ratio
+    plain / guided. Also reports the share of the plain error in pixels the
+    guide leaves unchanged (bit-identical in the first seed's two renders:
+    their paths reach no guided vertex). Prints one JSON line."""
     from sundog_b200 import scene as sc
     from sundog_b200 import workloads
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
     w, h, spp, ref_spp, seeds = 640, 360, args.guide_spp, args.guide_ref_spp, args.guide_seeds
     ad = asset_dir()
-    with sc.Session(workloads.volumes(ad, width=w, height=h, spp=ref_spp), base_dir=ad,
-                    seed=1000) as r:
+    if args.guide_scene == "volumes":
+        make = lambda n: workloads.volumes(ad, width=w, height=h, spp=n)
+        desc = ("flame + water + nested glass + rough panels + 2048-tri mesh light, 640x360 "
+                "(config-2 scene at reduced resolution)")
+    else:
+        make = lambda n: workloads.instancing(ad, width=w, height=h, spp=n)
+        desc = ("1024 displaced icosphere instances, Lambert / metal / plastic, sun-and-sky "
+                "env map, 640x360 (config-1 scene at reduced resolution)")
+    with sc.Session(make(ref_spp), base_dir=ad, seed=1000) as r:
         rr = r.render()
         ref = r.read()
-    s = workloads.volumes(ad, width=w, height=h, spp=spp)
-    out = {}
+    s = make(spp)
+    out, first = {}, {}
     for name, guided in (("plain", False), ("guided", True)):
-        errs, trimmed, ms, train_ms = [], [], [], []
+        errs, trimmed, ms, kms, train_ms = [], [], [], [], []
         for k in range(seeds):
             with sc.Session(s, base_dir=ad, seed=1 + k) as ses:
                 if guided:
@@ -453,29 +490,36 @@ def run_guiding(args):
                 img = ses.read()
                 if guided:
                     train_ms.append(ses.guiding_stats().train_ms)
+            if k == 0:
+                first[name] = img
             e, emap = _relmse(img, ref)
             errs.append(e)
             trimmed.append(float(np.sort(emap.ravel())[:int(emap.size * 0.999)].mean()))
             ms.append(res.render_ms)
+            kms.append(res.kernel_ms)
         out[name] = {"relmse_per_seed": errs, "relmse": float(np.mean(errs)),
                      "relmse_without_top_0.1pct": float(np.mean(trimmed)),
-                     "ms": float(np.mean(ms))}
+                     "ms": float(np.mean(ms)), "path_kernel_ms": float(np.mean(kms))}
         if guided:
             out[name]["train_ms"] = float(np.mean(train_ms))
+    same = np.all(first["plain"][..., :3] == first["guided"][..., :3], axis=-1)
+    _, emap = _relmse(first["plain"], ref)
     p, g = out["plain"], out["guided"]
     line = {
         "metric": "equal-time relMSE ratio plain / guided",
         "value": (p["relmse"] * p["ms"]) / (g["relmse"] * g["ms"]),
         "unit": "x", "higher_is_better": True, "n_gpus": 1,
         "dtype": "f32 render, bf16 network", "data": "synthetic",
-        "config": {"workload": "flame + water + nested glass + rough panels + 2048-tri mesh "
-                               "light, 640x360 (config-2 scene at reduced resolution)",
+        "config": {"workload": desc, "scene": args.guide_scene,
                    "spp": spp, "seeds": seeds, "reference_spp": ref_spp,
                    "relmse": "mean over pixels of (x - ref)^2 / (ref^2 + 0.01), RGB mean",
                    "equal_time": "relMSE x render time (MSE ~ 1/time for unbiased estimators)"},
         "equal_spp_ratio": p["relmse"] / g["relmse"],
         "equal_time_ratio_without_top_0.1pct_pixels":
             (p["relmse_without_top_0.1pct"] * p["ms"]) / (g["relmse_without_top_0.1pct"] * g["ms"]),
+        "time_ratio": g["ms"] / p["ms"],
+        "unguided_pixels": {"fraction": float(same.mean()),
+                            "share_of_plain_error": float(emap[same].sum() / emap.sum())},
         "plain": p, "guided": g, "reference_ms": rr.render_ms,
     }
     print(json.dumps(line))

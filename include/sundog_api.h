@@ -204,6 +204,12 @@ typedef struct {
                             persistent megakernel), 1 = persistent megakernel
                             throughout, 2 = same as 0. Both engines give the
                             same samples. */
+  int32_t shard_count;   /* > 1: render one tile shard of the frame, for one
+                            GPU of shard_count: the 64x64 film tiles t
+                            (row-major) with t % shard_count == shard_index.
+                            Those pixels equal the whole-frame render's bit
+                            for bit; the others stay 0. <= 1 = whole frame */
+  int32_t shard_index;
 } sundog_render_ext;
 
 typedef struct {
@@ -245,6 +251,12 @@ SUNDOG_API int sundog_session_render(sundog_session*, void* cuda_stream, int res
 SUNDOG_API int sundog_session_read(sundog_session*, float* film_rgba, float* aov_albedo,
                                    float* aov_normal);
 SUNDOG_API int sundog_session_info(sundog_session*, sundog_session_stats*);
+/* Device-to-device copy of the session's film (width*height float4 running
+ * means, device memory the caller owns) on cuda_stream (NULL = default
+ * stream); returns once the copy is queued. For gathering the tile shards of
+ * a frame rendered on several GPUs (shard_count in sundog_render_ext) with
+ * the caller's collective library. Returns 0/1. */
+SUNDOG_API int sundog_session_copy_film(sundog_session*, void* film_device, void* cuda_stream);
 SUNDOG_API void sundog_session_destroy(sundog_session*);
 
 /* Traversal visit counts over one full render of the session (a counting

@@ -55,7 +55,8 @@ class RenderExt(ctypes.Structure):
                 ("aov_normal", ctypes.c_void_p), ("chunk_spp", ctypes.c_int32),
                 ("repeat", ctypes.c_int32), ("guiding", ctypes.c_int32),
                 ("sample_offset", ctypes.c_int32), ("frame_spp", ctypes.c_int32),
-                ("engine", ctypes.c_int32)]
+                ("engine", ctypes.c_int32), ("shard_count", ctypes.c_int32),
+                ("shard_index", ctypes.c_int32)]
 
 
 class RenderResult(ctypes.Structure):
@@ -155,6 +156,7 @@ ADDITIVE_SYMBOLS = [
     "sundog_session_guide_records", "sundog_server_defaults", "sundog_server_create",
     "sundog_server_submit", "sundog_server_status", "sundog_server_wait",
     "sundog_server_cancel", "sundog_server_stats", "sundog_server_destroy",
+    "sundog_session_copy_film",
 ]
 
 _lib = None
@@ -215,6 +217,7 @@ def load(path=None):
     lib.sundog_session_render.argtypes = [vp, vp, ip, ctypes.POINTER(RenderResult)]
     lib.sundog_session_read.argtypes = [vp, vp, vp, vp]
     lib.sundog_session_info.argtypes = [vp, ctypes.POINTER(SessionStats)]
+    lib.sundog_session_copy_film.argtypes = [vp, vp, vp]
     lib.sundog_session_trace_counts.argtypes = [vp, ctypes.POINTER(TraceCounts)]
     lib.sundog_transfer_bytes.argtypes = [ctypes.POINTER(ctypes.c_uint64)] * 2
     lib.sundog_transfer_bytes.restype = None

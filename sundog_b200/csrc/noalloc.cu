@@ -152,6 +152,7 @@ extern "C" int sundog_session_render_tile_noalloc(sundog_session* sh, int x0, in
   unsigned char* base = (unsigned char*)scratchAddress();
 
   SdLaunch lp = s.lp;
+  lp.shardCount = 0;  // ids below use the whole-frame numbering
   lp.aovOn = 0;
   lp.sampleOffset = sample_begin;
   lp.sppThisLaunch = sample_count;

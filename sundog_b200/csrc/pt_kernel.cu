@@ -23,8 +23,16 @@ namespace sdb {
 
 __constant__ SdLaunch c_lp;
 
+// Resident blocks per SM of the training-record variants, whose per-path
+// trail of guided vertices adds to the path state.
+#ifndef SDB_RECORD_MIN_BLOCKS
+#define SDB_RECORD_MIN_BLOCKS SDB_MIN_BLOCKS
+#endif
+
 template <bool COUNT, int GUIDE>
-__global__ void __launch_bounds__(kRenderBlock, SDB_MIN_BLOCKS) ptPersistent(TraceCount* counts) {
+__global__ void __launch_bounds__(kRenderBlock, (GUIDE & kGuideRecord) ? SDB_RECORD_MIN_BLOCKS
+                                                                        : SDB_MIN_BLOCKS)
+    ptPersistent(TraceCount* counts) {
   const SdLaunch& lp = c_lp;
   TraceCount cnt = {0, 0, 0, 0, 0, 0, 0, 0};
   const unsigned full = 0xFFFFFFFFu;
@@ -91,6 +99,10 @@ __global__ void ptFold() {
   int npix = lp.width * lp.height;
   int pix = blockIdx.x * blockDim.x + threadIdx.x;
   if (pix >= npix) return;
+  if (lp.shardCount > 1) {  // another shard's pixel: no samples here
+    int px = pix % lp.width, py = pix / lp.width;
+    if (((py >> 6) * lp.shardTilesX + (px >> 6)) % lp.shardCount != lp.shardIndex) return;
+  }
   float4 acc = lp.accum[pix];
   for (int i = 0; i < lp.sppThisLaunch; i++) {
     float4 x = lp.sampleL[(size_t)i * npix + pix];
@@ -120,23 +132,35 @@ cudaError_t setLaunch(const SdLaunch& lp, cudaStream_t st) {
 
 int bvhWidth() { return SDB_WIDE_BVH ? 8 : 2; }
 
-int renderGridSize() {
+// Persistent grid of a path kernel: every SM filled with resident blocks.
+template <typename K>
+static int persistentGrid(K kernel) {
   int dev = 0, sms = 0, perSm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, ptPersistent<false, 0>, kRenderBlock, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kRenderBlock, 0);
   if (perSm < 1) perSm = 1;
   return sms * perSm;
 }
 
+int renderGridSize() { return persistentGrid(ptPersistent<false, 0>); }
+
+// grid: the plain kernel's persistent grid; the record variants size their
+// own (their register budget differs).
 cudaError_t launchRender(cudaStream_t st, int grid, int guide) {
   switch (guide) {
     case 0: ptPersistent<false, 0><<<grid, kRenderBlock, 0, st>>>(nullptr); break;
     case kGuideSample: ptPersistent<false, kGuideSample><<<grid, kRenderBlock, 0, st>>>(nullptr); break;
-    case kGuideRecord: ptPersistent<false, kGuideRecord><<<grid, kRenderBlock, 0, st>>>(nullptr); break;
-    case kGuideSample | kGuideRecord:
-      ptPersistent<false, kGuideSample | kGuideRecord><<<grid, kRenderBlock, 0, st>>>(nullptr);
+    case kGuideRecord: {
+      static const int g = persistentGrid(ptPersistent<false, kGuideRecord>);
+      ptPersistent<false, kGuideRecord><<<g, kRenderBlock, 0, st>>>(nullptr);
       break;
+    }
+    case kGuideSample | kGuideRecord: {
+      static const int g = persistentGrid(ptPersistent<false, kGuideSample | kGuideRecord>);
+      ptPersistent<false, kGuideSample | kGuideRecord><<<g, kRenderBlock, 0, st>>>(nullptr);
+      break;
+    }
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

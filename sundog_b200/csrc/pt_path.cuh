@@ -100,11 +100,22 @@ __device__ __forceinline__ void startPathAt(const SdLaunch& lp, int px, int py, 
 
 // Camera sample for path index id; false if the index is tile padding.
 __device__ __forceinline__ bool startPath(const SdLaunch& lp, unsigned long long id, Path& p) {
-  int sLocal = (int)(id / (unsigned long long)lp.npixPad);
-  int rem = (int)(id - (unsigned long long)sLocal * lp.npixPad);
-  int tile = rem >> 6, within = rem & 63;
-  int tx = tile % lp.tilesX, ty = tile / lp.tilesX;
-  int px = tx * 8 + (within & 7), py = ty * 8 + (within >> 3);
+  int sLocal, px, py;
+  if (lp.shardCount > 1) {
+    sLocal = (int)(id / (unsigned long long)lp.shardPad);
+    int rem = (int)(id - (unsigned long long)sLocal * lp.shardPad);
+    int tile = (rem >> 12) * lp.shardCount + lp.shardIndex;
+    int block = (rem >> 6) & 63, within = rem & 63;
+    px = (tile % lp.shardTilesX) * 64 + (block & 7) * 8 + (within & 7);
+    py = (tile / lp.shardTilesX) * 64 + (block >> 3) * 8 + (within >> 3);
+  } else {
+    sLocal = (int)(id / (unsigned long long)lp.npixPad);
+    int rem = (int)(id - (unsigned long long)sLocal * lp.npixPad);
+    int tile = rem >> 6, within = rem & 63;
+    int tx = tile % lp.tilesX, ty = tile / lp.tilesX;
+    px = tx * 8 + (within & 7);
+    py = ty * 8 + (within >> 3);
+  }
   if (px >= lp.width || py >= lp.height) return false;
   startPathAt(lp, px, py, lp.sampleOffset + sLocal, p);
   p.slot = sLocal * (lp.width * lp.height) + py * lp.width + px;

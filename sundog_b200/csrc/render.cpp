@@ -406,6 +406,10 @@ void DeviceScene::fillLaunch(SdLaunch& l) const {
   l.numInstances = numObjects;
 }
 
+// Paths per sample of a launch: the padded film, or the owned tiles of a
+// tile shard.
+static int pathsPerSample(const SdLaunch& l) { return l.shardCount > 1 ? l.shardPad : l.npixPad; }
+
 // Render settings and camera of one film (rs: settings after overrides).
 void fillRenderLaunch(SdLaunch& l, const SceneDesc& scene, const RenderCfg& rs) {
   l.width = rs.width;
@@ -507,6 +511,22 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
   std::memset(&l, 0, sizeof l);
   fillRenderLaunch(l, scene, rs);
   if (ext && ext->frame_spp > 0) l.nStrata = strataFor(ext->frame_spp);
+  shardPixels = npix;
+  if (ext && ext->shard_count > 1) {
+    const int n = ext->shard_count, r = ext->shard_index;
+    if (r < 0 || r >= n) throw std::runtime_error("render: shard_index must be in [0, shard_count)");
+    l.shardCount = n;
+    l.shardIndex = r;
+    l.shardTilesX = (rs.width + 63) / 64;
+    const int tiles = l.shardTilesX * ((rs.height + 63) / 64);
+    const int owned = r < tiles ? (tiles - r + n - 1) / n : 0;
+    l.shardPad = owned * 4096;
+    shardPixels = 0;
+    for (int t = r; t < tiles; t += n) {
+      int x0 = (t % l.shardTilesX) * 64, y0 = (t / l.shardTilesX) * 64;
+      shardPixels += (unsigned long long)std::min(64, rs.width - x0) * std::min(64, rs.height - y0);
+    }
+  }
   engine = ext ? ext->engine : 0;
   if (engine < 0 || engine > 2) throw std::runtime_error("render: engine must be 0, 1 or 2");
   dev->fillLaunch(l);
@@ -569,12 +589,14 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
     }
     lp.sampleOffset = sampleBase + done;
     lp.sppThisLaunch = n;
-    lp.numPaths = (unsigned long long)lp.npixPad * n;
+    lp.numPaths = (unsigned long long)pathsPerSample(lp) * n;
     cudaCheck(cudaMemsetAsync(lp.pathCounter, 0, sizeof(unsigned long long), st), "counter reset");
     cudaCheck(setLaunch(lp, st), "launch params");
     cudaCheck(cudaEventRecord(kev[0], st), "event");
     const bool wavefront = (mode == 0 || mode == kGuideSample) && engine != 1;
-    if (wavefront) {
+    if (lp.numPaths == 0) {
+      // A tile shard that owns no tile: nothing to trace.
+    } else if (wavefront) {
       if (!wf) wf = wfAcquire();
       wf->ensure((int)std::min<unsigned long long>(lp.numPaths, kWavefrontSlots));
       launches += wfRender(lp, *wf, st, mode);
@@ -607,12 +629,12 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
   lastKernelMs = evMs;
   if (res) {
     res->rays_traced = rays;
-    res->paths = (uint64_t)npix * lp.sppTotal;
+    res->paths = (uint64_t)shardPixels * lp.sppTotal;
     res->render_ms = wall;
     res->build_ms = buildMs;
     res->load_ms = loadMs;
     res->mrays_per_sec = wall > 0 ? rays / wall / 1000.0 : 0.0;
-    res->samples_per_sec = wall > 0 ? (double)npix * lp.sppTotal / (wall / 1000.0) : 0.0;
+    res->samples_per_sec = wall > 0 ? (double)shardPixels * lp.sppTotal / (wall / 1000.0) : 0.0;
     res->kernel_launches = launches;
     res->kernel_ms = kms;
   }
@@ -630,7 +652,7 @@ void RenderSession::countTraversal(sundog_trace_counts* out) {
     int n = std::min(chunk, lp.sppTotal - done);
     lp.sampleOffset = sampleBase + done;
     lp.sppThisLaunch = n;
-    lp.numPaths = (unsigned long long)lp.npixPad * n;
+    lp.numPaths = (unsigned long long)pathsPerSample(lp) * n;
     cudaCheck(cudaMemsetAsync(lp.pathCounter, 0, sizeof(unsigned long long), stream), "counter reset");
     cudaCheck(setLaunch(lp, stream), "launch params");
     cudaCheck(launchRenderCounting(stream, grid, (TraceCount*)dc.ptr), "counting launch");
@@ -732,6 +754,17 @@ extern "C" int sundog_session_read(sundog_session* sh, float* film, float* alb, 
   SDB_TRY
   if (!sh) throw std::runtime_error("session: null handle");
   reinterpret_cast<RenderSession*>(sh)->read(film, alb, nrm);
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_session_copy_film(sundog_session* sh, void* film_device, void* stream) {
+  SDB_TRY
+  if (!sh || !film_device) throw std::runtime_error("session: null argument");
+  RenderSession* s = reinterpret_cast<RenderSession*>(sh);
+  cudaCheck(cudaMemcpyAsync(film_device, s->accum.ptr, s->accum.bytes, cudaMemcpyDeviceToDevice,
+                            (cudaStream_t)stream),
+            "film copy");
   return SUNDOG_OK;
   SDB_CATCH(SUNDOG_ERROR)
 }

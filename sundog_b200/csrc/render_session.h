@@ -77,6 +77,7 @@ struct RenderSession {
   bool aov = false;
   int chunk = 1;
   int sampleBase = 0;  // first sample index of a render
+  unsigned long long shardPixels = 0;  // film pixels this session renders
   int grid = 0;
   size_t freeBefore = 0, deviceBytes = 0;
   size_t meshTriangles = 0, numNodes = 0, numTris = 0;

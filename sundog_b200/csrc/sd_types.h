@@ -154,6 +154,14 @@ struct SdLaunch {
   // work decomposition: path p -> (sample p / npixPad, tile-ordered pixel)
   int tilesX;
   int npixPad;
+  // Tile shard (one GPU of several): shardCount > 1 renders only the 64x64
+  // film tiles t (row-major over shardTilesX tiles across) with
+  // t % shardCount == shardIndex; path p -> (sample p / shardPad, owned tile,
+  // 8x8 block, pixel). Every pixel keeps the seeds of the whole-frame render.
+  int shardCount;
+  int shardIndex;
+  int shardTilesX;
+  int shardPad;          // owned tiles x 4096
   unsigned long long numPaths;
   unsigned long long* pathCounter;
   unsigned long long* rayCounter;

@@ -319,14 +319,15 @@ class Session(object):
     """A scene resident on the device (sundog_session_*)."""
 
     def __init__(self, scene, base_dir=".", aov=False, chunk_spp=0, guiding=0, sample_offset=0,
-                 frame_spp=0, engine=0, **opts):
+                 frame_spp=0, engine=0, shard_count=0, shard_index=0, **opts):
         self.lib = abi.load()
         h = scene.build(base_dir, self.lib)
         try:
             o = abi.options(**opts)
             dummy = np.zeros(4, np.float32)
             ext = abi.RenderExt(None, dummy.ctypes.data if aov else None, None, chunk_spp, 1,
-                                guiding, sample_offset, frame_spp, engine)
+                                guiding, sample_offset, frame_spp, engine, shard_count,
+                                shard_index)
             self.handle = self.lib.sundog_session_create(h, ctypes.byref(o), ctypes.byref(ext))
             if not self.handle:
                 raise abi.SundogError("session: " + abi.last_error(self.lib))
@@ -392,6 +393,12 @@ class Session(object):
         abi.check(self.lib.sundog_session_read(self.handle, film.ctypes.data, None, None), "read",
                   self.lib)
         return film
+
+    def copy_film(self, film_device_ptr, stream=None):
+        """Device-to-device copy of the film into caller-owned device memory
+        (width*height float4) on `stream` (a cudaStream_t as int)."""
+        abi.check(self.lib.sundog_session_copy_film(self.handle, film_device_ptr, stream),
+                  "copy film", self.lib)
 
     def close(self):
         if getattr(self, "handle", None):
