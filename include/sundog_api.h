@@ -199,11 +199,11 @@ typedef struct {
                             of: the pixel strata follow it, so blocks rendered
                             apart (one per GPU) hold exactly the frame's
                             samples; <= 0 = this render's spp */
-  int32_t engine;        /* path-tracing kernels: 0 = automatic (wavefront,
-                            except guiding's training passes, which run in the
-                            persistent megakernel), 1 = persistent megakernel
-                            throughout, 2 = same as 0. Both engines give the
-                            same samples. */
+  int32_t engine;        /* path-tracing kernels: 0 = automatic (the
+                            wavefront engine, guiding's training passes
+                            included), 1 = persistent megakernel throughout,
+                            2 = same as 0. Both engines give the same
+                            samples. */
   int32_t shard_count;   /* > 1: render one tile shard of the frame, for one
                             GPU of shard_count: the 64x64 film tiles t
                             (row-major) with t % shard_count == shard_index.
@@ -323,11 +323,11 @@ SUNDOG_API int sundog_selftest(int which, const void* in, int n, void* out,
  * the samples use the final guide. Every sample goes to the film. */
 typedef struct {
   int32_t train_spp;      /* samples whose paths train the network (32) */
-  int32_t pass_spp;       /* samples per training pass (4) */
+  int32_t pass_spp;       /* samples per training pass (8) */
   int32_t steps_per_pass; /* Adam steps after each pass (64) */
   int32_t batch;          /* training records per step (16384) */
   float learning_rate;    /* Adam step size (5e-3) */
-  float mix;              /* probability of drawing from the guide, [0, 1) (0.5) */
+  float mix;              /* probability of drawing from the guide, [0, 1) (0.7) */
   uint64_t seed;          /* network initialisation and batch draws (1) */
   uint64_t record_cap;    /* training records kept per pass (4194304) */
 } sundog_guiding_config;

@@ -877,11 +877,11 @@ sundog_guiding_config guideDefaults() {
   sundog_guiding_config c;
   std::memset(&c, 0, sizeof c);
   c.train_spp = 32;
-  c.pass_spp = 4;
+  c.pass_spp = 8;
   c.steps_per_pass = 64;
   c.batch = 16384;
   c.learning_rate = 5e-3f;
-  c.mix = 0.5f;
+  c.mix = 0.7f;
   c.seed = 1;
   c.record_cap = 1ull << 22;
   return c;

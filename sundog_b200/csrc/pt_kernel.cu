@@ -23,16 +23,8 @@ namespace sdb {
 
 __constant__ SdLaunch c_lp;
 
-// Resident blocks per SM of the training-record variants, whose per-path
-// trail of guided vertices adds to the path state.
-#ifndef SDB_RECORD_MIN_BLOCKS
-#define SDB_RECORD_MIN_BLOCKS SDB_MIN_BLOCKS
-#endif
-
 template <bool COUNT, int GUIDE>
-__global__ void __launch_bounds__(kRenderBlock, (GUIDE & kGuideRecord) ? SDB_RECORD_MIN_BLOCKS
-                                                                        : SDB_MIN_BLOCKS)
-    ptPersistent(TraceCount* counts) {
+__global__ void __launch_bounds__(kRenderBlock, SDB_MIN_BLOCKS) ptPersistent(TraceCount* counts) {
   const SdLaunch& lp = c_lp;
   TraceCount cnt = {0, 0, 0, 0, 0, 0, 0, 0};
   const unsigned full = 0xFFFFFFFFu;
@@ -146,7 +138,7 @@ static int persistentGrid(K kernel) {
 int renderGridSize() { return persistentGrid(ptPersistent<false, 0>); }
 
 // grid: the plain kernel's persistent grid; the record variants size their
-// own (their register budget differs).
+// own (their trail of guided vertices may change their occupancy).
 cudaError_t launchRender(cudaStream_t st, int grid, int guide) {
   switch (guide) {
     case 0: ptPersistent<false, 0><<<grid, kRenderBlock, 0, st>>>(nullptr); break;

@@ -593,7 +593,7 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
     cudaCheck(cudaMemsetAsync(lp.pathCounter, 0, sizeof(unsigned long long), st), "counter reset");
     cudaCheck(setLaunch(lp, st), "launch params");
     cudaCheck(cudaEventRecord(kev[0], st), "event");
-    const bool wavefront = (mode == 0 || mode == kGuideSample) && engine != 1;
+    const bool wavefront = engine != 1;
     if (lp.numPaths == 0) {
       // A tile shard that owns no tile: nothing to trace.
     } else if (wavefront) {

@@ -63,7 +63,9 @@ __device__ __forceinline__ unsigned long long nextPathId() {
 }
 
 // Puts the next camera path in `slot` and lists it in list `out`; leaves the
-// slot empty when the frame's paths are used up.
+// slot empty when the frame's paths are used up. Record passes (GUIDE &
+// kGuideRecord) start the slot's trail empty.
+template <int GUIDE>
 __device__ __forceinline__ void refill(int slot, int out) {
   const SdLaunch& lp = c_wlp;
   const WfPool& pool = c_pool;
@@ -73,14 +75,19 @@ __device__ __forceinline__ void refill(int slot, int out) {
     Path p;
     if (startPath(lp, id, p)) {
       pool.paths[slot] = p;
+      if (GUIDE & kGuideRecord) pool.trails[slot].n = 0;
       pool.lists[out][appendSlot(&pool.counts[out])] = slot;
       return;
     }
   }
 }
 
-__device__ __forceinline__ void finishPath(const Path& p) {
+// The finished path's sample; record passes also turn its trail of guided
+// vertices into training records.
+template <int GUIDE>
+__device__ __forceinline__ void finishPath(const Path& p, int slot) {
   float3 L = sanitize3(p.L);
+  if (GUIDE & kGuideRecord) guideFlush(c_wlp, c_pool.trails[slot], L);
   c_wlp.sampleL[p.slot] = make_float4(L.x, L.y, L.z, 1.0f);
 }
 
@@ -89,11 +96,12 @@ __device__ __forceinline__ void addRays(unsigned long long rays) {
   if ((threadIdx.x & 31) == 0 && rays) atomicAdd(c_wlp.rayCounter, rays);
 }
 
+template <int GUIDE>
 __global__ void __launch_bounds__(kRenderBlock) wfStart() {
   const WfPool& pool = c_pool;
   for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < pool.cap;
        slot += gridDim.x * blockDim.x)
-    refill(slot, 0);
+    refill<GUIDE>(slot, 0);
 }
 
 __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTrace(int in) {
@@ -115,6 +123,7 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTrace(int
   addRays(rays);
 }
 
+template <int GUIDE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeA(int in, int out) {
   const SdLaunch& lp = c_wlp;
   const WfPool& pool = c_pool;
@@ -131,9 +140,9 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeA(in
       pool.pending[slot] = 1;
       if (v.nee) pool.shadowList[appendSlot(&pool.counts[2])] = slot;
     } else {
-      finishPath(p);
+      finishPath<GUIDE>(p, slot);
       pool.pending[slot] = 0;
-      refill(slot, out);
+      refill<GUIDE>(slot, out);
     }
   }
   addRays(rays);
@@ -151,8 +160,9 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfShadow() 
   }
 }
 
-// GUIDE = kGuideSample: the BSDF sample by MIS with the learned guide
-// (sd_guide.cuh); the mixture table is in the launch block.
+// GUIDE & kGuideSample: the BSDF sample by MIS with the learned guide
+// (sd_guide.cuh; the mixture table is in the launch block). GUIDE &
+// kGuideRecord: the guided vertex joins the slot's trail.
 template <int GUIDE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeB(int in, int out) {
   const SdLaunch& lp = c_wlp;
@@ -168,12 +178,13 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeB(in
       float4 t4 = pool.trs[slot];
       tr = v3(t4.x, t4.y, t4.z);
     }
-    if (finishVertex<GUIDE>(lp, p, v, tr)) {
+    GuideTrail* trail = (GUIDE & kGuideRecord) ? &pool.trails[slot] : nullptr;
+    if (finishVertex<GUIDE>(lp, p, v, tr, trail)) {
       pool.paths[slot] = p;
       pool.lists[out][appendSlot(&pool.counts[out])] = slot;
     } else {
-      finishPath(p);
-      refill(slot, out);
+      finishPath<GUIDE>(p, slot);
+      refill<GUIDE>(slot, out);
     }
   }
 }
@@ -203,10 +214,16 @@ void WfBuffers::ensure(int slots) {
   if (!hostCount) cudaCheck(cudaMallocHost((void**)&hostCount, sizeof(unsigned)), "pinned count");
   cap = slots;
   gridTrace = gridFor(wfTrace);
-  gridShadeA = gridFor(wfShadeA);
+  gridShadeA = gridFor(wfShadeA<0>);
   gridShadow = gridFor(wfShadow);
   gridShadeB = gridFor(wfShadeB<0>);
-  gridStart = gridFor(wfStart);
+  gridStart = gridFor(wfStart<0>);
+}
+
+void WfBuffers::ensureTrails() {
+  if (trailCap >= cap) return;
+  trails.alloc((size_t)cap * sizeof(GuideTrail));
+  trailCap = cap;
 }
 
 WfBuffers::~WfBuffers() {
@@ -241,9 +258,19 @@ size_t wfSlotBytes() {
 
 // Renders the launch block's paths (lp.numPaths ids, counters already
 // cleared) into lp.sampleL through the stages. Returns the kernels launched.
+// One iteration's stage kernels for guide mode GUIDE.
+template <int GUIDE>
+static void wfIteration(const WfBuffers& b, cudaStream_t st, int cur, int nxt) {
+  wfTrace<<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
+  wfShadeA<GUIDE><<<b.gridShadeA, kRenderBlock, 0, st>>>(cur, nxt);
+  wfShadow<<<b.gridShadow, kRenderBlock, 0, st>>>();
+  wfShadeB<GUIDE><<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
+}
+
 int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
-  if (guide != 0 && guide != kGuideSample)
-    throw std::runtime_error("wavefront: training passes run in the persistent kernel");
+  if (guide < 0 || guide > (kGuideSample | kGuideRecord))
+    throw std::runtime_error("wavefront: invalid guide mode");
+  if (guide & kGuideRecord) b.ensureTrails();
   WfPool pool;
   pool.paths = (Path*)b.paths.ptr;
   pool.verts = (Vertex*)b.verts.ptr;
@@ -254,6 +281,7 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
   pool.lists[1] = (int*)b.list1.ptr;
   pool.shadowList = (int*)b.shadow.ptr;
   pool.counts = (unsigned*)b.counts.ptr;
+  pool.trails = (GuideTrail*)b.trails.ptr;
   pool.cap = (int)std::min<unsigned long long>((unsigned long long)b.cap, lp.numPaths);
   cudaCheck(cudaMemcpyToSymbolAsync(c_wlp, &lp, sizeof lp, 0, cudaMemcpyHostToDevice, st),
             "wavefront launch block");
@@ -261,7 +289,10 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
             "wavefront pool");
   cudaCheck(cudaMemsetAsync(b.counts.ptr, 0, b.counts.bytes, st), "wavefront counts");
   int launches = 0;
-  wfStart<<<b.gridStart, kRenderBlock, 0, st>>>();
+  if (guide & kGuideRecord)
+    wfStart<kGuideRecord><<<b.gridStart, kRenderBlock, 0, st>>>();
+  else
+    wfStart<0><<<b.gridStart, kRenderBlock, 0, st>>>();
   cudaCheck(cudaGetLastError(), "wfStart");
   launches++;
   unsigned* counts = (unsigned*)b.counts.ptr;
@@ -270,13 +301,12 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
     int nxt = 1 - cur;
     cudaCheck(cudaMemsetAsync(counts + nxt, 0, sizeof(unsigned), st), "wavefront counts");
     cudaCheck(cudaMemsetAsync(counts + 2, 0, sizeof(unsigned), st), "wavefront counts");
-    wfTrace<<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
-    wfShadeA<<<b.gridShadeA, kRenderBlock, 0, st>>>(cur, nxt);
-    wfShadow<<<b.gridShadow, kRenderBlock, 0, st>>>();
-    if (guide == kGuideSample)
-      wfShadeB<kGuideSample><<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
-    else
-      wfShadeB<0><<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
+    switch (guide) {
+      case 0: wfIteration<0>(b, st, cur, nxt); break;
+      case kGuideSample: wfIteration<kGuideSample>(b, st, cur, nxt); break;
+      case kGuideRecord: wfIteration<kGuideRecord>(b, st, cur, nxt); break;
+      default: wfIteration<kGuideSample | kGuideRecord>(b, st, cur, nxt); break;
+    }
     cudaCheck(cudaGetLastError(), "wavefront stage");
     launches += 4;
     cur = nxt;

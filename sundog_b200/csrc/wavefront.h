@@ -13,6 +13,7 @@ namespace sdb {
 struct Path;
 struct Vertex;
 struct TraceHit;
+struct GuideTrail;
 
 // Device view of the slot pool (one path per slot).
 struct WfPool {
@@ -24,20 +25,24 @@ struct WfPool {
   int* lists[2];           // live slot lists, ping-pong between iterations
   int* shadowList;
   unsigned* counts;        // [0], [1]: list lengths; [2]: shadow-list length
+  GuideTrail* trails;      // guided vertices awaiting their path's end (record passes)
   int cap;
 };
 
 // Host-owned pool storage, grown on demand.
 struct WfBuffers {
   DevBuf paths, verts, hits, trs, pending, list0, list1, shadow, counts;
+  DevBuf trails;  // allocated by the first training-record pass
   unsigned* hostCount = nullptr;
   int cap = 0;
+  int trailCap = 0;
   int gridStart = 0, gridTrace = 0, gridShadeA = 0, gridShadow = 0, gridShadeB = 0;
   WfBuffers() = default;
   WfBuffers(const WfBuffers&) = delete;
   WfBuffers& operator=(const WfBuffers&) = delete;
   ~WfBuffers();
   void ensure(int slots);
+  void ensureTrails();  // one GuideTrail per slot
 };
 
 // Device bytes per pool slot.
@@ -48,9 +53,10 @@ std::unique_ptr<WfBuffers> wfAcquire();
 void wfRelease(std::unique_ptr<WfBuffers> b);
 // Renders lp.numPaths camera paths (counters cleared by the caller) into
 // lp.sampleL; returns the number of kernels launched. Synchronises st once per
-// iteration to read the live-path count. guide: 0, or kGuideSample to draw
-// directions by MIS with the learned guide of lp (training passes, which keep
-// per-path records, run in the persistent kernel).
+// iteration to read the live-path count. guide: 0, or a combination of
+// kGuideSample (draw directions by MIS with the learned guide of lp) and
+// kGuideRecord (keep each path's guided vertices in its slot's trail and turn
+// them into training records when the path ends).
 int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide = 0);
 
 }  // namespace sdb
