@@ -1,6 +1,7 @@
 // Binned SAH build (Wald, "On fast Construction of SAH-based Bounding Volume
 // Hierarchies", 2007): 32 bins per axis over centroid bounds, all three axes
-// evaluated, leaf when splitting costs more than intersecting; below the
+// binned in one pass, ranges of up to 32 primitives split exactly over their
+// sorted centroids, leaf when splitting costs more than intersecting; below the
 // depth limit of 48 a median split guarantees termination, so a traversal
 // stack of 64 entries covers TLAS + BLAS depth.
 #include "bvh_build.h"
@@ -12,14 +13,20 @@
 
 namespace sdb {
 
+// Plain comparisons rather than fminf / fmaxf, which the host compiler
+// calls out of line (NaN rules) at this optimisation level: the builder's
+// bounds are finite.
+static inline float minOf(float a, float b) { return b < a ? b : a; }
+static inline float maxOf(float a, float b) { return b > a ? b : a; }
+
 Box3 boxEmpty() { return {v3(FLT_MAX), v3(-FLT_MAX)}; }
 void boxGrow(Box3& b, float3 p) {
-  b.lo = vmin(b.lo, p);
-  b.hi = vmax(b.hi, p);
+  b.lo = v3(minOf(b.lo.x, p.x), minOf(b.lo.y, p.y), minOf(b.lo.z, p.z));
+  b.hi = v3(maxOf(b.hi.x, p.x), maxOf(b.hi.y, p.y), maxOf(b.hi.z, p.z));
 }
 void boxGrow(Box3& b, const Box3& o) {
-  b.lo = vmin(b.lo, o.lo);
-  b.hi = vmax(b.hi, o.hi);
+  b.lo = v3(minOf(b.lo.x, o.lo.x), minOf(b.lo.y, o.lo.y), minOf(b.lo.z, o.lo.z));
+  b.hi = v3(maxOf(b.hi.x, o.hi.x), maxOf(b.hi.y, o.hi.y), maxOf(b.hi.z, o.hi.z));
 }
 static float boxArea(const Box3& b) {
   float3 e = b.hi - b.lo;
@@ -30,6 +37,7 @@ static float boxArea(const Box3& b) {
 namespace {
 
 constexpr int kBins = 32;
+constexpr int kSmall = 32;  // ranges up to this size are split exactly
 constexpr int kDepthLimit = 40;
 
 struct Builder {
@@ -60,8 +68,121 @@ struct Builder {
     return ~code;
   }
 
-  // Returns the split position in [b+1, e-1], or -1 for a leaf.
-  int split(int b, int e, int depth) {
+  // Sorts ids[b, e) by centroid along ax (insertion sort: small ranges only;
+  // ties keep their order, so the result is deterministic).
+  void sortSmall(int b, int e, int ax) {
+    for (int i = b + 1; i < e; i++) {
+      int id = ids[i];
+      float key = comp(cent[id], ax);
+      int j = i - 1;
+      while (j >= b && comp(cent[ids[j]], ax) > key) {
+        ids[j + 1] = ids[j];
+        j--;
+      }
+      ids[j + 1] = id;
+    }
+  }
+
+  // Best SAH split of a small range: every position along each axis's
+  // centroid order. Returns the cost; ax / pos the split (pos = primitives
+  // on the left), ax = -1 if no axis has extent.
+  float exactSweep(int b, int e, const float3& ext, int& bestAx, int& bestPos) {
+    const int n = e - b;
+    float bestCost = FLT_MAX;
+    bestAx = -1;
+    float rightA[kSmall];
+    for (int ax = 0; ax < 3; ax++) {
+      if (!(comp(ext, ax) > 0.0f)) continue;
+      sortSmall(b, e, ax);
+      Box3 acc = boxEmpty();
+      for (int i = n - 1; i > 0; i--) {
+        boxGrow(acc, boxes[ids[b + i]]);
+        rightA[i] = boxArea(acc);
+      }
+      acc = boxEmpty();
+      for (int i = 1; i < n; i++) {
+        boxGrow(acc, boxes[ids[b + i - 1]]);
+        float c = boxArea(acc) * i + rightA[i] * (n - i);
+        if (c < bestCost) {
+          bestCost = c;
+          bestAx = ax;
+          bestPos = i;
+        }
+      }
+    }
+    return bestCost;
+  }
+
+  // Binned SAH over all three axes in one pass over the primitives. Returns
+  // the cost; ax / bin the split (bins <= bin go left), ax = -1 if none.
+  float binnedSweep(int b, int e, const Box3& cb, const float3& ext, int& bestAx, int& bestBin,
+                    Box3& lb, Box3& rb) {
+    Box3 bb[3][kBins];
+    int bc[3][kBins];
+    float lo[3], sc[3];
+    bool on[3];
+    for (int ax = 0; ax < 3; ax++) {
+      on[ax] = comp(ext, ax) > 0.0f;
+      lo[ax] = comp(cb.lo, ax);
+      sc[ax] = on[ax] ? kBins / comp(ext, ax) : 0.0f;
+      for (int k = 0; k < kBins; k++) {
+        bb[ax][k] = boxEmpty();
+        bc[ax][k] = 0;
+      }
+    }
+    for (int i = b; i < e; i++) {
+      const int id = ids[i];
+      const Box3& bx = boxes[id];
+      const float3 c = cent[id];
+      for (int ax = 0; ax < 3; ax++) {
+        if (!on[ax]) continue;
+        int k = (int)((comp(c, ax) - lo[ax]) * sc[ax]);
+        k = std::min(std::max(k, 0), kBins - 1);
+        bc[ax][k]++;
+        boxGrow(bb[ax][k], bx);
+      }
+    }
+    float bestCost = FLT_MAX;
+    bestAx = -1;
+    for (int ax = 0; ax < 3; ax++) {
+      if (!on[ax]) continue;
+      float rightA[kBins];
+      int rightN[kBins];
+      Box3 acc = boxEmpty();
+      int cnt = 0;
+      for (int k = kBins - 1; k > 0; k--) {
+        boxGrow(acc, bb[ax][k]);
+        cnt += bc[ax][k];
+        rightA[k] = boxArea(acc);
+        rightN[k] = cnt;
+      }
+      acc = boxEmpty();
+      cnt = 0;
+      for (int k = 0; k < kBins - 1; k++) {
+        boxGrow(acc, bb[ax][k]);
+        cnt += bc[ax][k];
+        if (cnt == 0 || rightN[k + 1] == 0) continue;
+        float c = boxArea(acc) * cnt + rightA[k + 1] * rightN[k + 1];
+        if (c < bestCost) {
+          bestCost = c;
+          bestAx = ax;
+          bestBin = k;
+        }
+      }
+    }
+    if (bestAx >= 0) {
+      lb = boxEmpty();
+      rb = boxEmpty();
+      for (int k = 0; k < kBins; k++) boxGrow(k <= bestBin ? lb : rb, bb[bestAx][k]);
+    }
+    return bestCost;
+  }
+
+  // Returns the split position in [b+1, e-1] with the two children's bounds
+  // in lb / rb, or -1 for a leaf. nb: the bounds of [b, e). Ranges of up to
+  // kSmall primitives are split exactly (every centroid position), larger
+  // ones by binning; the child bounds come from the sweep itself.
+  int split(int b, int e, int depth, const Box3& nb, Box3& lb, Box3& rb) {
     int n = e - b;
     if (n <= 1) return -1;
     Box3 cb = boxEmpty();
@@ -69,56 +190,19 @@ struct Builder {
     float3 ext = cb.hi - cb.lo;
     bool forceMedian = depth >= kDepthLimit;
     float bestCost = FLT_MAX;
-    int bestAxis = -1, bestBin = -1;
+    int bestAx = -1, bestAt = -1;
     if (!forceMedian) {
-      for (int ax = 0; ax < 3; ax++) {
-        float lo = comp(cb.lo, ax), e0 = comp(ext, ax);
-        if (!(e0 > 0.0f)) continue;
-        Box3 bb[kBins];
-        int bc[kBins];
-        for (int k = 0; k < kBins; k++) {
-          bb[k] = boxEmpty();
-          bc[k] = 0;
-        }
-        float sc = kBins / e0;
-        for (int i = b; i < e; i++) {
-          int k = (int)((comp(cent[ids[i]], ax) - lo) * sc);
-          k = std::min(std::max(k, 0), kBins - 1);
-          bc[k]++;
-          boxGrow(bb[k], boxes[ids[i]]);
-        }
-        float rightA[kBins];
-        int rightN[kBins];
-        Box3 acc = boxEmpty();
-        int cnt = 0;
-        for (int k = kBins - 1; k > 0; k--) {
-          boxGrow(acc, bb[k]);
-          cnt += bc[k];
-          rightA[k] = boxArea(acc);
-          rightN[k] = cnt;
-        }
-        acc = boxEmpty();
-        cnt = 0;
-        for (int k = 0; k < kBins - 1; k++) {
-          boxGrow(acc, bb[k]);
-          cnt += bc[k];
-          if (cnt == 0 || rightN[k + 1] == 0) continue;
-          float c = boxArea(acc) * cnt + rightA[k + 1] * rightN[k + 1];
-          if (c < bestCost) {
-            bestCost = c;
-            bestAxis = ax;
-            bestBin = k;
-          }
-        }
-      }
+      if (n <= kSmall)
+        bestCost = exactSweep(b, e, ext, bestAx, bestAt);
+      else
+        bestCost = binnedSweep(b, e, cb, ext, bestAx, bestAt, lb, rb);
     }
-    Box3 nb = rangeBox(b, e);
     float leafCost = boxArea(nb) * n;
     const float kTraverse = 1.2f;  // node visit relative to one primitive test
-    if (!forceMedian && bestAxis >= 0 && n <= maxLeaf &&
+    if (!forceMedian && bestAx >= 0 && n <= maxLeaf &&
         leafCost <= bestCost + kTraverse * boxArea(nb))
       return -1;
-    if (bestAxis < 0) {
+    if (bestAx < 0) {
       if (n <= maxLeaf) return -1;
       // Degenerate centroids or depth limit: median split on the widest axis.
       int ax = ext.x >= ext.y && ext.x >= ext.z ? 0 : (ext.y >= ext.z ? 1 : 2);
@@ -126,29 +210,42 @@ struct Builder {
       std::nth_element(ids.begin() + b, ids.begin() + mid, ids.begin() + e, [&](int x, int y) {
         return comp(cent[x], ax) < comp(cent[y], ax);
       });
+      lb = rangeBox(b, mid);
+      rb = rangeBox(mid, e);
       return mid;
     }
-    float lo = comp(cb.lo, bestAxis), sc = kBins / comp(ext, bestAxis);
+    if (n <= kSmall) {
+      sortSmall(b, e, bestAx);
+      int mid = b + bestAt;
+      lb = rangeBox(b, mid);
+      rb = rangeBox(mid, e);
+      return mid;
+    }
+    float lo = comp(cb.lo, bestAx), sc = kBins / comp(ext, bestAx);
     int* pm = std::partition(ids.data() + b, ids.data() + e, [&](int id) {
-      int k = (int)((comp(cent[id], bestAxis) - lo) * sc);
+      int k = (int)((comp(cent[id], bestAx) - lo) * sc);
       k = std::min(std::max(k, 0), kBins - 1);
-      return k <= bestBin;
+      return k <= bestAt;
     });
     int mid = (int)(pm - ids.data());
-    if (mid == b || mid == e) mid = b + n / 2;
+    if (mid == b || mid == e) {
+      mid = b + n / 2;
+      lb = rangeBox(b, mid);
+      rb = rangeBox(mid, e);
+    }
     return mid;
   }
 
-  // Encoded link for [b, e).
-  int build(int b, int e, int depth) {
+  // Encoded link for [b, e) with bounds nb.
+  int build(int b, int e, int depth, const Box3& nb) {
     out.maxDepth = std::max(out.maxDepth, depth);
-    int m = split(b, e, depth);
+    Box3 lb, rb;
+    int m = split(b, e, depth, nb, lb, rb);
     if (m < 0) return leafLink(b, e);
     int idx = (int)out.nodes.size();
     out.nodes.push_back(BvhNode{});
-    Box3 lb = rangeBox(b, m), rb = rangeBox(m, e);
-    int l = build(b, m, depth + 1);
-    int r = build(m, e, depth + 1);
+    int l = build(b, m, depth + 1, lb);
+    int r = build(m, e, depth + 1, rb);
     fill(out.nodes[idx], lb, rb, l, r);
     return nodeBase + idx;
   }
@@ -173,14 +270,15 @@ BvhBuild buildBvh(const std::vector<Box3>& boxes, int maxLeaf, int nodeBase, int
     Builder::fill(bd.out.nodes[0], far, far, ~0, ~0);
     return bd.out;
   }
-  int m = bd.split(0, n, 0);
+  const Box3 root = bd.rangeBox(0, n);
+  Box3 lb, rb;
+  int m = bd.split(0, n, 0, root, lb, rb);
   if (m < 0) {
     Box3 far = {v3(3e30f), v3(3e30f)};
-    Builder::fill(bd.out.nodes[0], bd.rangeBox(0, n), far, bd.leafLink(0, n), bd.leafLink(0, n));
+    Builder::fill(bd.out.nodes[0], root, far, bd.leafLink(0, n), bd.leafLink(0, n));
   } else {
-    Box3 lb = bd.rangeBox(0, m), rb = bd.rangeBox(m, n);
-    int l = bd.build(0, m, 1);
-    int r = bd.build(m, n, 1);
+    int l = bd.build(0, m, 1, lb);
+    int r = bd.build(m, n, 1, rb);
     Builder::fill(bd.out.nodes[0], lb, rb, l, r);
   }
   bd.out.order = bd.ids;
@@ -200,19 +298,20 @@ struct BinBuilder {
   BinTree out;
   BinBuilder(const std::vector<Box3>& b, int ml) : core(b, ml, 0, 0) {}
 
-  int build(int b, int e, int depth) {
+  int build(int b, int e, int depth, const Box3& nb) {
     out.maxDepth = std::max(out.maxDepth, depth);
     int idx = (int)out.nodes.size();
     out.nodes.push_back(BinNode{});
-    out.nodes[idx].box = core.rangeBox(b, e);
-    int m = core.split(b, e, depth);
+    out.nodes[idx].box = nb;
+    Box3 lb, rb;
+    int m = core.split(b, e, depth, nb, lb, rb);
     if (m < 0) {
       out.nodes[idx].start = b;
       out.nodes[idx].count = e - b;
       return idx;
     }
-    int l = build(b, m, depth + 1);
-    int r = build(m, e, depth + 1);
+    int l = build(b, m, depth + 1, lb);
+    int r = build(m, e, depth + 1, rb);
     out.nodes[idx].left = l;
     out.nodes[idx].right = r;
     return idx;
@@ -271,7 +370,7 @@ uint8_t quantHi(float p, int e, float v) {
 
 BinTree buildBinary(const std::vector<Box3>& boxes, int maxLeaf) {
   BinBuilder bb(boxes, maxLeaf);
-  if (!boxes.empty()) bb.build(0, (int)boxes.size(), 0);
+  if (!boxes.empty()) bb.build(0, (int)boxes.size(), 0, bb.core.rangeBox(0, (int)boxes.size()));
   bb.out.order = bb.core.ids;
   return bb.out;
 }

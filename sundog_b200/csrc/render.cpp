@@ -105,7 +105,7 @@ void buildEnvCdf(const float* rgba, int w, int h, std::vector<float>& marg, std:
     for (int col = 0; col < w; col++) {
       const float* p = rgba + 4 * ((size_t)row * w + col);
       float lum = 0.2126f * p[0] + 0.7152f * p[1] + 0.0722f * p[2];
-      sum += (double)fmaxf(lum, 0.0f) * sinT;
+      sum += (double)(lum > 0.0f ? lum : 0.0f) * sinT;  // fmaxf(lum, 0), NaN -> 0
       cdf[col + 1] = (float)sum;
     }
     if (sum > 0.0) {
