@@ -1,13 +1,13 @@
 // Wavefront path tracer: the plain path kernel's per-path computation split
 // into stages over a pool of path slots held in global memory.
 //
-//   wfStart    fill every slot with a camera path
+//   wfStart        fill every slot with a camera path
 //   per iteration, over the slots in the live list:
-//   wfTrace    trace the radiance ray (traversal only)
-//   wfShadeA   shadeVertex: media, flames, escape, shading, emission, the NEE
-//              light draw; queues the slot's shadow ray
-//   wfShadow   trace the queued shadow rays (transparent-shadow traversal)
-//   wfShadeB   finishVertex: NEE contribution, BSDF sample, roulette
+//   wfTraceFetch   trace the radiance ray (traversal only)
+//   wfShadeA       shadeVertex: media, flames, escape, shading, emission, the
+//                  NEE light draw; queues the slot's shadow ray
+//   wfShadow       trace the queued shadow rays (transparent shadows)
+//   wfShadeB       finishVertex: NEE contribution, BSDF sample, roulette
 //
 // A slot whose path ends writes that sample and takes the next camera path at
 // once (warp-aggregated counter), so the pool stays full until the frame's
@@ -104,21 +104,181 @@ __global__ void __launch_bounds__(kRenderBlock) wfStart() {
     refill<GUIDE>(slot, 0);
 }
 
-__global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTrace(int in) {
+// Idle lanes a warp gathers before it fetches new rays (measured on the
+// instancing frame: 894 Mrays/s at 24, 869 with a grid-stride loop, 752 when
+// every idle lane fetches at once: fresh rays at the TLAS root diverge from
+// the warp's deep BLAS walks).
+#ifndef SDB_WF_FETCH_IDLE
+#define SDB_WF_FETCH_IDLE 24
+#endif
+
+// Radiance rays with dynamic ray fetch (Aila and Laine, "Understanding the
+// Efficiency of Ray Traversal on GPUs", 2009): the traversal loop runs per
+// warp, and a lane whose ray is done writes its hit and, once
+// SDB_WF_FETCH_IDLE lanes of the warp are idle, takes the next ray of the
+// live list (one warp-aggregated atomicAdd on counts[3]), so a warp no longer
+// waits for its longest ray. Each ray visits the nodes of traverse<false>
+// (sd_trace.cuh) in the same order with the same tests: the same closest
+// accepted hit. (Shadow rays, shorter, gained nothing from it.)
+__global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetch(int in) {
   const SdLaunch& lp = c_wlp;
   const WfPool& pool = c_pool;
   const unsigned n = pool.counts[in];
+  const unsigned full = 0xFFFFFFFFu;
+  const unsigned ltMask = (1u << (threadIdx.x & 31)) - 1u;
+  const BvhNode* nodes = lp.nodes;
+  const float tmin = 0.0f;
   unsigned long long rays = 0;
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int slot = pool.lists[in][i];
-    const Path& p = pool.paths[slot];
-    TraceHit h;
-    float dummyTr = 1.0f;
-    float3 dummyTau = v3(0.0f);
-    bool hit = traverse<false, false>(lp, p.o, p.d, 1e16f, h, dummyTr, dummyTau, nullptr);
-    if (!hit) h.inst = -1;
-    pool.hits[slot] = h;
-    rays++;
+  int slot = -1;
+  bool exhausted = false;  // warp-uniform
+  float3 O = v3(0.0f), D = v3(0.0f), ro = v3(0.0f), rd = v3(0.0f), id = v3(0.0f), oi = v3(0.0f);
+  WtRay wr;
+  float tmax = 0.0f;
+  TraceHit hit;
+  bool found = false, inBlas = false;
+  int curInst = -1, cur = kPop, sp = 0;
+  int stack[kStackSize];
+  while (true) {
+    const unsigned idle = __ballot_sync(full, slot < 0);
+    if (!exhausted && (idle == full || __popc(idle) >= SDB_WF_FETCH_IDLE)) {
+      const int leader = __ffs(idle) - 1;
+      unsigned base = 0;
+      if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&pool.counts[3], (unsigned)__popc(idle));
+      base = __shfl_sync(full, base, leader);
+      if (base + __popc(idle) >= n) exhausted = true;
+      if (slot < 0) {
+        unsigned i = base + __popc(idle & ltMask);
+        if (i < n) {
+          slot = pool.lists[in][i];
+          O = pool.paths[slot].o;
+          D = pool.paths[slot].d;
+          ro = O;
+          rd = D;
+          id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
+          oi = ro * id;
+          tmax = 1e16f;
+          found = false;
+          inBlas = false;
+          curInst = -1;
+          sp = 0;
+          cur = lp.numInstances > 0 ? lp.tlasRoot : kPop;
+        }
+      }
+    }
+    if (__ballot_sync(full, slot >= 0) == 0) {
+      if (exhausted) break;
+      continue;
+    }
+    if (slot < 0) continue;
+    if (cur >= 0) {
+      BvhNode nd = loadNode(nodes, cur);
+      float ta, tb;
+      bool ha, hb;
+      boxPair(nd, oi, id, tmin, tmax, ta, tb, ha, hb);
+      if (ha && hb) {
+        int first = nd.link.x, second = nd.link.y;
+        if (tb < ta) {
+          first = nd.link.y;
+          second = nd.link.x;
+        }
+        if (sp < kStackSize) stack[sp++] = second;
+        cur = first;
+      } else if (ha) {
+        cur = nd.link.x;
+      } else if (hb) {
+        cur = nd.link.y;
+      } else {
+        cur = kPop;
+      }
+      continue;
+    }
+    if (cur == kPop) {
+      if (sp == 0) {  // ray done
+        if (!found) hit.inst = -1;
+        pool.hits[slot] = hit;
+        rays++;
+        slot = -1;
+        continue;
+      }
+      cur = stack[--sp];
+      if (cur == kToTlas) {
+        inBlas = false;
+        ro = O;
+        rd = D;
+        id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
+        oi = ro * id;
+        cur = kPop;
+      }
+      continue;
+    }
+    // Leaf: ~cur = start << 3 | (count - 1).
+    const int code = ~cur;
+    const int start = code >> 3;
+    const int count = (code & 7) + 1;
+    cur = kPop;
+    if (!inBlas) {
+      // TLAS leaves hold exactly one instance.
+      const SdInstance& inst = lp.inst[start];
+      float3 o2 = xfPoint(inst.w2o, O), d2 = xfVec(inst.w2o, D);
+      if (inst.kind == GK_MESH) {
+        if (sp < kStackSize) {
+          stack[sp++] = kToTlas;
+          inBlas = true;
+          curInst = start;
+          ro = o2;
+          rd = d2;
+          id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
+          oi = ro * id;
+          wr = wtSetup(rd);
+          cur = lp.meshes[inst.mesh].root;
+        }
+        continue;
+      }
+      QHits qh = hitQuadric(inst.kind, o2, d2, tmin, tmax);
+      for (int k = 0; k < qh.n; k++) {
+        const QHit& q = qh.h[k];
+        if (q.t >= tmax) continue;
+        bool front = dot(q.n, d2) < 0.0f;
+        if ((inst.flags & kInstMasked) && !faceAccepts(lp, inst, front, q.u, q.v)) continue;
+        tmax = q.t;
+        found = true;
+        hit.t = q.t;
+        hit.inst = start;
+        hit.prim = 0;
+        hit.u = q.u;
+        hit.v = q.v;
+        hit.nq = q.n;
+        hit.front = front;
+      }
+      continue;
+    }
+    // BLAS leaf: triangles in object space of curInst.
+    for (int k = 0; k < count; k++) {
+      const float4* tp = lp.tris + 3 * (size_t)(start + k);
+      float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+      float t, b1, b2;
+      float3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
+      if (!wtHit(wr, ro, p0, p1, p2, tmin, tmax, t, b1, b2)) continue;
+      int prim = __float_as_int(a.w);
+      const SdInstance& inst = lp.inst[curInst];
+      bool needFace = (inst.flags & (kInstMasked | kInstTransmissive)) != 0;
+      bool front;
+      if (!needFace) {
+        front = dot(cross(p1 - p0, p2 - p0), rd) < 0.0f;
+      } else {
+        ShadePt spt = triShade(lp, inst, prim, b1, b2, D);
+        if ((inst.flags & kInstMasked) && !faceAccepts(lp, inst, spt.front, spt.u, spt.v)) continue;
+        front = spt.front;
+      }
+      tmax = t;
+      found = true;
+      hit.t = t;
+      hit.inst = curInst;
+      hit.prim = prim;
+      hit.u = b1;
+      hit.v = b2;
+      hit.front = front;
+    }
   }
   addRays(rays);
 }
@@ -213,7 +373,7 @@ void WfBuffers::ensure(int slots) {
   if (!counts.ptr) counts.alloc(4 * sizeof(unsigned));
   if (!hostCount) cudaCheck(cudaMallocHost((void**)&hostCount, sizeof(unsigned)), "pinned count");
   cap = slots;
-  gridTrace = gridFor(wfTrace);
+  gridTrace = gridFor(wfTraceFetch);
   gridShadeA = gridFor(wfShadeA<0>);
   gridShadow = gridFor(wfShadow);
   gridShadeB = gridFor(wfShadeB<0>);
@@ -261,7 +421,7 @@ size_t wfSlotBytes() {
 // One iteration's stage kernels for guide mode GUIDE.
 template <int GUIDE>
 static void wfIteration(const WfBuffers& b, cudaStream_t st, int cur, int nxt) {
-  wfTrace<<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
+  wfTraceFetch<<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
   wfShadeA<GUIDE><<<b.gridShadeA, kRenderBlock, 0, st>>>(cur, nxt);
   wfShadow<<<b.gridShadow, kRenderBlock, 0, st>>>();
   wfShadeB<GUIDE><<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
@@ -300,7 +460,7 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
   for (int iter = 0;; iter++) {
     int nxt = 1 - cur;
     cudaCheck(cudaMemsetAsync(counts + nxt, 0, sizeof(unsigned), st), "wavefront counts");
-    cudaCheck(cudaMemsetAsync(counts + 2, 0, sizeof(unsigned), st), "wavefront counts");
+    cudaCheck(cudaMemsetAsync(counts + 2, 0, 2 * sizeof(unsigned), st), "wavefront counts");
     switch (guide) {
       case 0: wfIteration<0>(b, st, cur, nxt); break;
       case kGuideSample: wfIteration<kGuideSample>(b, st, cur, nxt); break;

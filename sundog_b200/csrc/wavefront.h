@@ -24,7 +24,8 @@ struct WfPool {
   unsigned char* pending;  // 1: the slot's second half is due this iteration
   int* lists[2];           // live slot lists, ping-pong between iterations
   int* shadowList;
-  unsigned* counts;        // [0], [1]: list lengths; [2]: shadow-list length
+  unsigned* counts;        // [0], [1]: list lengths; [2]: shadow-list length;
+                           // [3]: rays the trace stage has fetched
   GuideTrail* trails;      // guided vertices awaiting their path's end (record passes)
   int cap;
 };
