@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -150,7 +151,34 @@ static int strataFor(int spp) {  // device/programs.cu:317-319
   return n;
 }
 
+// One idle per-sample radiance buffer per device, kept between sessions: a
+// one-shot render (sundog_render, sundog_render_ex) would otherwise allocate
+// and free about 1 GiB per call (the free alone measured 5-60 ms).
+static std::mutex g_samplesMu;
+static DevBuf g_idleSamples[64];
+
+static void acquireSamples(DevBuf& b, size_t bytes) {
+  int dev = 0;
+  cudaCheck(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev >= 0 && dev < 64) {
+    std::lock_guard<std::mutex> lock(g_samplesMu);
+    if (g_idleSamples[dev].ptr && g_idleSamples[dev].bytes >= bytes) {
+      b = std::move(g_idleSamples[dev]);
+      return;
+    }
+  }
+  b.alloc(bytes);
+}
+
+static void releaseSamples(DevBuf& b) {
+  int dev = 0;
+  if (!b.ptr || cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(g_samplesMu);
+  if (g_idleSamples[dev].bytes < b.bytes) g_idleSamples[dev] = std::move(b);
+}
+
 RenderSession::~RenderSession() {
+  releaseSamples(sampleL);
   wfRelease(std::move(wf));
   if (stream) cudaStreamDestroy(stream);
   if (ev0) cudaEventDestroy(ev0);
@@ -500,7 +528,7 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
   }
   chunk = std::min(chunk, rs.spp);
   sampleBase = ext && ext->sample_offset > 0 ? ext->sample_offset : 0;
-  sampleL.alloc(npix * chunk * sizeof(float4));
+  acquireSamples(sampleL, npix * chunk * sizeof(float4));
   if (aov) {
     sampleAlb.alloc(npix * chunk * sizeof(float4));
     sampleNrm.alloc(npix * chunk * sizeof(float4));

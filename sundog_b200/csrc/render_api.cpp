@@ -179,9 +179,14 @@ int renderImpl(sundog_scene* h, const sundog_render_options* opt, const sundog_r
   }
   r = bestR;
   size_t npix = (size_t)rs.width * rs.height;
-  std::vector<float> film(npix * 4);
-  s->read(film.data(), nullptr, nullptr);
-  if (ext && ext->film_rgba) std::memcpy(ext->film_rgba, film.data(), film.size() * sizeof(float));
+  // The film goes straight into the caller's buffer when there is one.
+  std::vector<float> own;
+  float* film = ext && ext->film_rgba ? ext->film_rgba : nullptr;
+  if (!film) {
+    own.resize(npix * 4);
+    film = own.data();
+  }
+  s->read(film, nullptr, nullptr);
   std::vector<float> alb, nrm;
   if (s->aov) {
     alb.resize(npix * 4);
@@ -192,7 +197,7 @@ int renderImpl(sundog_scene* h, const sundog_render_options* opt, const sundog_r
   }
   float scale = exp2f(rs.exposure);
   if (opt->out_path && *opt->out_path) {
-    std::string wrote = writeImage(opt->out_path, film.data(), rs.width, rs.height, scale);
+    std::string wrote = writeImage(opt->out_path, film, rs.width, rs.height, scale);
     if (opt->aov_albedo_path) writeImage(opt->aov_albedo_path, alb.data(), rs.width, rs.height, 1.0f);
     if (opt->aov_normal_path) writeImage(opt->aov_normal_path, nrm.data(), rs.width, rs.height, 1.0f);
     if (!quiet) {

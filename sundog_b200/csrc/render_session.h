@@ -24,6 +24,16 @@ struct DevBuf {
     o.ptr = nullptr;
     o.bytes = 0;
   }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      ptr = o.ptr;
+      bytes = o.bytes;
+      o.ptr = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
   ~DevBuf() { release(); }
   void alloc(size_t n);
   void upload(const void* src, size_t n);
