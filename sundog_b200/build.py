@@ -29,7 +29,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
                      "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
                      "-Xptxas", "-warn-spills"]
-CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off",
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-pthread", "-fvisibility=hidden", "-ffp-contract=off",
              "-Wall", "-Wno-unused-function", "-I" + os.path.join(CUDA_HOME, "include")]
 
 
@@ -90,7 +90,7 @@ def build(verbose=False, force=False, defines=(), out=None):
             if verbose and out.strip():
                 print(out)
         objs.append(obj)
-    link = [NVCC] + ARCH + ["-shared", "-o", lib_path] + objs + ["-cudart", "static",
+    link = [NVCC] + ARCH + ["-shared", "-o", lib_path] + objs + ["-cudart", "static", "-lpthread",
                                                                "-Xlinker", "-soname=libsundog.so"]
     _run(link, verbose)
     return lib_path

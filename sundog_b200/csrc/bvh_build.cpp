@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <future>
 #include <cmath>
 #include <cstring>
 
@@ -40,22 +41,40 @@ constexpr int kBins = 32;
 constexpr int kSmall = 32;  // ranges up to this size are split exactly
 constexpr int kDepthLimit = 40;
 
-struct Builder {
-  const std::vector<Box3>& boxes;
+// Subtrees of at least kParallelMin primitives down to depth kParallelDepth
+// build their right half on another thread; the halves own disjoint ranges
+// of `ids`, and the right half's nodes are appended after the left's with
+// their links relocated, so the tree is the one the sequential build makes.
+constexpr int kParallelMin = 1024;
+constexpr int kParallelDepth = 3;
+
+// Primitive centroids and the primitive order, shared by a build's threads.
+struct BuildInput {
   std::vector<float3> cent;
   std::vector<int> ids;
-  int maxLeaf, nodeBase, primBase;
-  BvhBuild out;
-
-  Builder(const std::vector<Box3>& b, int ml, int nb, int pb)
-      : boxes(b), maxLeaf(ml), nodeBase(nb), primBase(pb) {
-    cent.resize(b.size());
-    ids.resize(b.size());
+  explicit BuildInput(const std::vector<Box3>& b) : cent(b.size()), ids(b.size()) {
     for (size_t i = 0; i < b.size(); i++) {
       cent[i] = (b[i].lo + b[i].hi) * 0.5f;
       ids[i] = (int)i;
     }
   }
+};
+
+struct Builder {
+  const std::vector<Box3>& boxes;
+  const std::vector<float3>& cent;
+  std::vector<int>& ids;
+  int maxLeaf, nodeBase, primBase;
+  bool parallel;
+  BvhBuild out;
+
+  Builder(const std::vector<Box3>& b, BuildInput& in, int ml, int nb, int pb, bool par)
+      : boxes(b), cent(in.cent), ids(in.ids), maxLeaf(ml), nodeBase(nb), primBase(pb),
+        parallel(par) {}
+  // A builder for a subtree of the same build, numbering its nodes from nb.
+  Builder(const Builder& o, int nb)
+      : boxes(o.boxes), cent(o.cent), ids(o.ids), maxLeaf(o.maxLeaf), nodeBase(nb),
+        primBase(o.primBase), parallel(o.parallel) {}
 
   Box3 rangeBox(int b, int e) const {
     Box3 r = boxEmpty();
@@ -244,10 +263,33 @@ struct Builder {
     if (m < 0) return leafLink(b, e);
     int idx = (int)out.nodes.size();
     out.nodes.push_back(BvhNode{});
-    int l = build(b, m, depth + 1, lb);
-    int r = build(m, e, depth + 1, rb);
+    int l, r;
+    children(b, m, e, depth + 1, lb, rb, l, r);
     fill(out.nodes[idx], lb, rb, l, r);
     return nodeBase + idx;
+  }
+
+  // Links of the children [b, m) and [m, e) at `depth`, left subtree first.
+  void children(int b, int m, int e, int depth, const Box3& lb, const Box3& rb, int& l, int& r) {
+    if (!parallel || e - b < kParallelMin || depth > kParallelDepth) {
+      l = build(b, m, depth, lb);
+      r = build(m, e, depth, rb);
+      return;
+    }
+    Builder sub(*this, 0);
+    std::future<int> right = std::async(std::launch::async, [&sub, m, e, depth, &rb] {
+      return sub.build(m, e, depth, rb);
+    });
+    l = build(b, m, depth, lb);
+    int rs = right.get();
+    const int off = nodeBase + (int)out.nodes.size();
+    for (BvhNode& nd : sub.out.nodes) {
+      if (nd.link.x >= 0) nd.link.x += off;
+      if (nd.link.y >= 0) nd.link.y += off;
+    }
+    r = rs >= 0 ? rs + off : rs;
+    out.nodes.insert(out.nodes.end(), sub.out.nodes.begin(), sub.out.nodes.end());
+    out.maxDepth = std::max(out.maxDepth, sub.out.maxDepth);
   }
 
   static void fill(BvhNode& nd, const Box3& a, const Box3& c, int la, int lc) {
@@ -261,7 +303,8 @@ struct Builder {
 }  // namespace
 
 BvhBuild buildBvh(const std::vector<Box3>& boxes, int maxLeaf, int nodeBase, int primBase) {
-  Builder bd(boxes, std::min(std::max(maxLeaf, 1), 8), nodeBase, primBase);
+  BuildInput in(boxes);
+  Builder bd(boxes, in, std::min(std::max(maxLeaf, 1), 8), nodeBase, primBase, true);
   int n = (int)boxes.size();
   bd.out.nodes.push_back(BvhNode{});  // root slot
   if (n == 0) {
@@ -277,8 +320,8 @@ BvhBuild buildBvh(const std::vector<Box3>& boxes, int maxLeaf, int nodeBase, int
     Box3 far = {v3(3e30f), v3(3e30f)};
     Builder::fill(bd.out.nodes[0], root, far, bd.leafLink(0, n), bd.leafLink(0, n));
   } else {
-    int l = bd.build(0, m, 1, lb);
-    int r = bd.build(m, n, 1, rb);
+    int l, r;
+    bd.children(0, m, n, 1, lb, rb, l, r);
     Builder::fill(bd.out.nodes[0], lb, rb, l, r);
   }
   bd.out.order = bd.ids;
@@ -294,9 +337,10 @@ namespace sdb {
 namespace {
 
 struct BinBuilder {
+  BuildInput in;
   Builder core;
   BinTree out;
-  BinBuilder(const std::vector<Box3>& b, int ml) : core(b, ml, 0, 0) {}
+  BinBuilder(const std::vector<Box3>& b, int ml) : in(b), core(b, in, ml, 0, 0, false) {}
 
   int build(int b, int e, int depth, const Box3& nb) {
     out.maxDepth = std::max(out.maxDepth, depth);

@@ -17,6 +17,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/sundog_api.h"
@@ -92,30 +93,43 @@ static void invertAffine(const Xform& x, float4 out[3]) {
 
 // Equirect CDFs over luminance * sin(theta), FP64 prefix sums stored as
 // float with the last entry pinned to 1; all-black rows get a uniform ramp.
-// (src/env_light.cpp:27-56)
+// (src/env_light.cpp:27-56) Rows are independent and run on several host
+// threads; the marginal prefix over the rows' sums stays sequential, so the
+// tables are bit-identical to a one-thread loop.
 void buildEnvCdf(const float* rgba, int w, int h, std::vector<float>& marg, std::vector<float>& cond,
                  bool& degenerate) {
   marg.assign(h + 1, 0.0f);
   cond.assign((size_t)h * (w + 1), 0.0f);
+  std::vector<double> rowSum(h, 0.0);
+  auto rows = [&](int r0, int r1) {
+    for (int row = r0; row < r1; row++) {
+      float sinT = sinf(kPi * (row + 0.5f) / h);
+      float* cdf = &cond[(size_t)row * (w + 1)];
+      double sum = 0.0;
+      cdf[0] = 0.0f;
+      for (int col = 0; col < w; col++) {
+        const float* p = rgba + 4 * ((size_t)row * w + col);
+        float lum = 0.2126f * p[0] + 0.7152f * p[1] + 0.0722f * p[2];
+        sum += (double)(lum > 0.0f ? lum : 0.0f) * sinT;  // fmaxf(lum, 0), NaN -> 0
+        cdf[col + 1] = (float)sum;
+      }
+      if (sum > 0.0) {
+        for (int c = 1; c <= w; c++) cdf[c] = (float)(cdf[c] / sum);
+      } else {
+        for (int c = 0; c <= w; c++) cdf[c] = (float)c / w;
+      }
+      cdf[w] = 1.0f;
+      rowSum[row] = sum;
+    }
+  };
+  const int nt = std::max(1, std::min({8, (int)std::thread::hardware_concurrency(), h / 64}));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; t++) pool.emplace_back(rows, (int)((long)h * t / nt), (int)((long)h * (t + 1) / nt));
+  rows(0, h / nt);
+  for (std::thread& th : pool) th.join();
   double total = 0.0;
   for (int row = 0; row < h; row++) {
-    float sinT = sinf(kPi * (row + 0.5f) / h);
-    float* cdf = &cond[(size_t)row * (w + 1)];
-    double sum = 0.0;
-    cdf[0] = 0.0f;
-    for (int col = 0; col < w; col++) {
-      const float* p = rgba + 4 * ((size_t)row * w + col);
-      float lum = 0.2126f * p[0] + 0.7152f * p[1] + 0.0722f * p[2];
-      sum += (double)(lum > 0.0f ? lum : 0.0f) * sinT;  // fmaxf(lum, 0), NaN -> 0
-      cdf[col + 1] = (float)sum;
-    }
-    if (sum > 0.0) {
-      for (int c = 1; c <= w; c++) cdf[c] = (float)(cdf[c] / sum);
-    } else {
-      for (int c = 0; c <= w; c++) cdf[c] = (float)c / w;
-    }
-    cdf[w] = 1.0f;
-    total += sum;
+    total += rowSum[row];
     marg[row + 1] = (float)total;
   }
   degenerate = total <= 0.0;
