@@ -68,8 +68,8 @@ def _run(cmd, verbose):
 
 def build(verbose=False, force=False, defines=(), out=None):
     """Compile every translation unit (cached by content hash) and link.
-    `defines` adds -D flags to the CUDA units (kernel tuning experiments);
-    `out` overrides the output library path."""
+    `defines` adds -D flags to every unit (tuning experiments); `out`
+    overrides the output library path."""
     lib_path = out or LIB
     os.makedirs(os.path.dirname(lib_path), exist_ok=True)
     os.makedirs(OBJ_DIR, exist_ok=True)
@@ -78,7 +78,7 @@ def build(verbose=False, force=False, defines=(), out=None):
     for src in _sources():
         path = os.path.join(CSRC, src)
         is_cu = src.endswith(".cu")
-        flags = (NVCC_FLAGS + ["-D" + d for d in defines]) if is_cu else CXX_FLAGS
+        flags = (NVCC_FLAGS if is_cu else CXX_FLAGS) + ["-D" + d for d in defines]
         tag = _digest(path, flags + [hdr])
         obj = os.path.join(OBJ_DIR, "%s.%s.o" % (src, tag))
         if force or not os.path.exists(obj):

@@ -588,9 +588,14 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
   setupMs = msSince(tTotal);
 }
 
-// Wavefront pool size (slots): 4 M (about 1.3 GB) keeps every stage launch full.
+// Wavefront pool size (slots, 285 B each; WfBuffers::ensure also caps it at
+// half the free device memory): up to 64 M, so a 32-spp chunk of a 1080p
+// frame (66 M paths) is almost all in flight at once and runs in about as
+// many iterations as its longest path has bounces. Measured on the instancing
+// frame: 894 / 981 / 1,049 / 1,092 / 1,115 Mrays/s at 4 / 8 / 16 / 32 / 64 M
+// slots (fewer iterations: fewer host round trips and stage-launch tails).
 #ifndef SDB_WF_SLOTS_LOG2
-#define SDB_WF_SLOTS_LOG2 22
+#define SDB_WF_SLOTS_LOG2 26
 #endif
 static constexpr unsigned long long kWavefrontSlots = 1ull << SDB_WF_SLOTS_LOG2;
 

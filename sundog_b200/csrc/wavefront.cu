@@ -41,10 +41,11 @@ __constant__ WfPool c_pool;
 #define SDB_WF_TRACE_BLOCKS 8
 #endif
 // Resident blocks per SM the stage kernels are compiled for (measured on the
-// instancing frame: traversal 8 -> 64 registers; shading 4 -> 128 registers,
-// 871 Mrays/s against 807-861 for 12/16 traversal or 8/16 shading blocks).
+// instancing frame with a 64 M-slot pool: traversal 8 -> 64 registers,
+// shading 5 -> 102 registers, 1,136 Mrays/s against 1,115 at 4 shading
+// blocks; 877 / 835 / 842 at 6 / 10 / 12 traversal blocks with 4 M slots).
 #ifndef SDB_WF_SHADE_BLOCKS
-#define SDB_WF_SHADE_BLOCKS 4
+#define SDB_WF_SHADE_BLOCKS 5
 #endif
 
 // Slot index for an append to a list by the calling lanes together.
@@ -361,6 +362,15 @@ static int gridFor(K kernel) {
 }
 
 void WfBuffers::ensure(int slots) {
+  if (slots <= cap) return;
+  // At most half of the device memory that is free (counting the pool about
+  // to be replaced), so films, scenes and other work keep room; at least
+  // 1 M slots.
+  size_t freeB = 0, totB = 0;
+  cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
+  const size_t budget = (freeB + (size_t)cap * wfSlotBytes()) / 2;
+  const size_t fit = std::max<size_t>(budget / wfSlotBytes(), (size_t)1 << 20);
+  slots = (int)std::min<size_t>((size_t)slots, fit);
   if (slots <= cap) return;
   paths.alloc((size_t)slots * sizeof(Path));
   verts.alloc((size_t)slots * sizeof(Vertex));
