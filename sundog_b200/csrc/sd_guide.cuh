@@ -37,11 +37,12 @@ namespace sdb {
 
 constexpr int kGuidePending = 4;
 
-struct GuideVertex {
+// 16-byte aligned like the other per-slot records of the wavefront engine.
+struct __align__(16) GuideVertex {
   float3 x, n, wi, beta, L;
   float pdf;
 };
-struct GuideTrail {
+struct __align__(16) GuideTrail {
   GuideVertex v[kGuidePending];
   int n;
 };
