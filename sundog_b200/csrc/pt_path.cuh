@@ -41,7 +41,7 @@ __device__ __forceinline__ float3 shadowTransmittance(const SdLaunch& lp, float3
   return tr;
 }
 
-struct __align__(16) Path {
+struct Path {
   float3 o, d, beta, L, prevX;
   float prevPdf;
   Pcg rng;
@@ -135,7 +135,7 @@ __device__ __forceinline__ void writeAov(const SdLaunch& lp, const Path& p, floa
 
 // State of a surface vertex between the two halves of a path segment: the
 // shading point, and the next-event estimate waiting for its shadow ray.
-struct __align__(16) Vertex {
+struct Vertex {
   float3 x, ns, albedo;
   float etaExt, etaRel;
   int matId;

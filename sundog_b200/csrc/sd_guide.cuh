@@ -37,12 +37,11 @@ namespace sdb {
 
 constexpr int kGuidePending = 4;
 
-// 16-byte aligned like the other per-slot records of the wavefront engine.
-struct __align__(16) GuideVertex {
+struct GuideVertex {
   float3 x, n, wi, beta, L;
   float pdf;
 };
-struct __align__(16) GuideTrail {
+struct GuideTrail {
   GuideVertex v[kGuidePending];
   int n;
 };

@@ -32,11 +32,7 @@ constexpr int kStackSize = 64;
 constexpr int kPop = (int)0x80000000;        // "take the next stack entry"
 constexpr int kToTlas = (int)0x80000001;     // marker: leave the BLAS
 
-// The records the wavefront engine keeps per path slot (TraceHit, Path,
-// Vertex) are 16-byte aligned, so the stages move them with 128-bit loads
-// and stores (instancing frame: 1,213 Mrays/s against 1,133 at their natural
-// 8-byte alignment, 1,158 at 32 bytes).
-struct __align__(16) TraceHit {
+struct TraceHit {
   float t;
   int inst;
   int prim;      // mesh-local triangle index (meshes)

@@ -75,8 +75,8 @@ __device__ __forceinline__ void refill(int slot, int out) {
     if (id >= lp.numPaths) return;
     Path p;
     if (startPath(lp, id, p)) {
-      pool.paths[slot] = p;
-      if (GUIDE & kGuideRecord) pool.trails[slot].n = 0;
+      pool.paths[slot].v = p;
+      if (GUIDE & kGuideRecord) pool.trails[slot].v.n = 0;
       pool.lists[out][appendSlot(&pool.counts[out])] = slot;
       return;
     }
@@ -88,7 +88,7 @@ __device__ __forceinline__ void refill(int slot, int out) {
 template <int GUIDE>
 __device__ __forceinline__ void finishPath(const Path& p, int slot) {
   float3 L = sanitize3(p.L);
-  if (GUIDE & kGuideRecord) guideFlush(c_wlp, c_pool.trails[slot], L);
+  if (GUIDE & kGuideRecord) guideFlush(c_wlp, c_pool.trails[slot].v, L);
   c_wlp.sampleL[p.slot] = make_float4(L.x, L.y, L.z, 1.0f);
 }
 
@@ -151,8 +151,8 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
         unsigned i = base + __popc(idle & ltMask);
         if (i < n) {
           slot = pool.lists[in][i];
-          O = pool.paths[slot].o;
-          D = pool.paths[slot].d;
+          O = pool.paths[slot].v.o;
+          D = pool.paths[slot].v.d;
           ro = O;
           rd = D;
           id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
     if (cur == kPop) {
       if (sp == 0) {  // ray done
         if (!found) hit.inst = -1;
-        pool.hits[slot] = hit;
+        pool.hits[slot].v = hit;
         rays++;
         slot = -1;
         continue;
@@ -292,12 +292,12 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeA(in
   unsigned long long rays = 0;
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int slot = pool.lists[in][i];
-    Path p = pool.paths[slot];
-    TraceHit h = pool.hits[slot];
+    Path p = pool.paths[slot].v;
+    TraceHit h = pool.hits[slot].v;
     Vertex v;
     if (shadeVertex<false>(lp, p, h.inst >= 0, h, rays, v)) {
-      pool.paths[slot] = p;
-      pool.verts[slot] = v;
+      pool.paths[slot].v = p;
+      pool.verts[slot].v = v;
       pool.pending[slot] = 1;
       if (v.nee) pool.shadowList[appendSlot(&pool.counts[2])] = slot;
     } else {
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfShadow() 
   const unsigned n = pool.counts[2];
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int slot = pool.shadowList[i];
-    const Vertex& v = pool.verts[slot];
+    const Vertex& v = pool.verts[slot].v;
     float3 tr = shadowTransmittance<false>(lp, v.so, v.wi, v.tmaxS, nullptr);
     pool.trs[slot] = make_float4(tr.x, tr.y, tr.z, 0.0f);
   }
@@ -332,16 +332,16 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeB(in
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int slot = pool.lists[in][i];
     if (!pool.pending[slot]) continue;
-    Path p = pool.paths[slot];
-    const Vertex v = pool.verts[slot];
+    Path p = pool.paths[slot].v;
+    const Vertex v = pool.verts[slot].v;
     float3 tr = v3(0.0f);
     if (v.nee) {
       float4 t4 = pool.trs[slot];
       tr = v3(t4.x, t4.y, t4.z);
     }
-    GuideTrail* trail = (GUIDE & kGuideRecord) ? &pool.trails[slot] : nullptr;
+    GuideTrail* trail = (GUIDE & kGuideRecord) ? &pool.trails[slot].v : nullptr;
     if (finishVertex<GUIDE>(lp, p, v, tr, trail)) {
-      pool.paths[slot] = p;
+      pool.paths[slot].v = p;
       pool.lists[out][appendSlot(&pool.counts[out])] = slot;
     } else {
       finishPath<GUIDE>(p, slot);
@@ -372,9 +372,9 @@ void WfBuffers::ensure(int slots) {
   const size_t fit = std::max<size_t>(budget / wfSlotBytes(), (size_t)1 << 20);
   slots = (int)std::min<size_t>((size_t)slots, fit);
   if (slots <= cap) return;
-  paths.alloc((size_t)slots * sizeof(Path));
-  verts.alloc((size_t)slots * sizeof(Vertex));
-  hits.alloc((size_t)slots * sizeof(TraceHit));
+  paths.alloc((size_t)slots * sizeof(PoolSlot<Path>));
+  verts.alloc((size_t)slots * sizeof(PoolSlot<Vertex>));
+  hits.alloc((size_t)slots * sizeof(PoolSlot<TraceHit>));
   trs.alloc((size_t)slots * sizeof(float4));
   pending.alloc((size_t)slots);
   list0.alloc((size_t)slots * sizeof(int));
@@ -392,7 +392,7 @@ void WfBuffers::ensure(int slots) {
 
 void WfBuffers::ensureTrails() {
   if (trailCap >= cap) return;
-  trails.alloc((size_t)cap * sizeof(GuideTrail));
+  trails.alloc((size_t)cap * sizeof(PoolSlot<GuideTrail>));
   trailCap = cap;
 }
 
@@ -423,7 +423,8 @@ void wfRelease(std::unique_ptr<WfBuffers> b) {
 }
 
 size_t wfSlotBytes() {
-  return sizeof(Path) + sizeof(Vertex) + sizeof(TraceHit) + sizeof(float4) + 1 + 3 * sizeof(int);
+  return sizeof(PoolSlot<Path>) + sizeof(PoolSlot<Vertex>) + sizeof(PoolSlot<TraceHit>) +
+         sizeof(float4) + 1 + 3 * sizeof(int);
 }
 
 // Renders the launch block's paths (lp.numPaths ids, counters already
@@ -442,16 +443,16 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
     throw std::runtime_error("wavefront: invalid guide mode");
   if (guide & kGuideRecord) b.ensureTrails();
   WfPool pool;
-  pool.paths = (Path*)b.paths.ptr;
-  pool.verts = (Vertex*)b.verts.ptr;
-  pool.hits = (TraceHit*)b.hits.ptr;
+  pool.paths = (PoolSlot<Path>*)b.paths.ptr;
+  pool.verts = (PoolSlot<Vertex>*)b.verts.ptr;
+  pool.hits = (PoolSlot<TraceHit>*)b.hits.ptr;
   pool.trs = (float4*)b.trs.ptr;
   pool.pending = (unsigned char*)b.pending.ptr;
   pool.lists[0] = (int*)b.list0.ptr;
   pool.lists[1] = (int*)b.list1.ptr;
   pool.shadowList = (int*)b.shadow.ptr;
   pool.counts = (unsigned*)b.counts.ptr;
-  pool.trails = (GuideTrail*)b.trails.ptr;
+  pool.trails = (PoolSlot<GuideTrail>*)b.trails.ptr;
   pool.cap = (int)std::min<unsigned long long>((unsigned long long)b.cap, lp.numPaths);
   cudaCheck(cudaMemcpyToSymbolAsync(c_wlp, &lp, sizeof lp, 0, cudaMemcpyHostToDevice, st),
             "wavefront launch block");

@@ -15,18 +15,28 @@ struct Vertex;
 struct TraceHit;
 struct GuideTrail;
 
+// A pool entry: the per-path record at a 16-byte boundary, so the stages
+// move it with 128-bit loads and stores (instancing frame: 1,213 Mrays/s
+// against 1,133 at the records' natural 8-byte alignment, 1,158 at 32
+// bytes). The records themselves keep their natural layout, so the
+// megakernel's register and local-memory frames do not grow.
+template <typename T>
+struct __align__(16) PoolSlot {
+  T v;
+};
+
 // Device view of the slot pool (one path per slot).
 struct WfPool {
-  Path* paths;
-  Vertex* verts;
-  TraceHit* hits;
+  PoolSlot<Path>* paths;
+  PoolSlot<Vertex>* verts;
+  PoolSlot<TraceHit>* hits;
   float4* trs;             // shadow-ray transmittance of the slot's vertex
   unsigned char* pending;  // 1: the slot's second half is due this iteration
   int* lists[2];           // live slot lists, ping-pong between iterations
   int* shadowList;
   unsigned* counts;        // [0], [1]: list lengths; [2]: shadow-list length;
                            // [3]: rays the trace stage has fetched
-  GuideTrail* trails;      // guided vertices awaiting their path's end (record passes)
+  PoolSlot<GuideTrail>* trails;  // guided vertices awaiting their path's end (record passes)
   int cap;
 };
 
