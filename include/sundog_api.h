@@ -385,16 +385,20 @@ SUNDOG_API int sundog_guide_gradients(const float* params, const float* records,
  * iteration is one persistent launch over tile-passes (a tile x tile pixel
  * rectangle and a range of its samples) drawn from every active job, then one
  * fold of those samples into each job's film. Jobs arriving while others run
- * join at the next iteration. A job's film is bit-identical to a
+ * join at the next iteration. A job's film is the same alone or in any mix
+ * of jobs, bit for bit; with engine 1 it is bit-identical to a
  * sundog_session_render of the same scene, size, spp and seed with the
- * megakernel engine (sundog_render_ext.engine = 1), alone or in any mix. */
+ * megakernel engine (sundog_render_ext.engine = 1), and with engine 0 it
+ * equals the wavefront engine's session render up to FP32 rounding (the same
+ * per-path code compiled into other kernels). */
 typedef struct sundog_server sundog_server;
 typedef struct {
   int32_t max_jobs;            /* jobs on the device at once, 1..32 (16) */
   int32_t tile;                /* tile edge in pixels, a multiple of 8 (64) */
   int32_t pass_spp;            /* samples of a tile per tile-pass (8) */
-  int32_t reserved0;
-  uint64_t iteration_paths;    /* camera paths per launch (8388608) */
+  int32_t engine;              /* path-tracing kernels: 0 = wavefront (default),
+                                  1 = persistent megakernel, 2 = same as 0 */
+  uint64_t iteration_paths;    /* camera paths per batch (8388608) */
   uint64_t reserve_bytes;      /* device memory left free at admission (1 GiB) */
   uint64_t scene_cache_bytes;  /* scene data kept resident with no job using it (8 GiB) */
 } sundog_server_config;

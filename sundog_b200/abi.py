@@ -102,7 +102,7 @@ class GuidingStats(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("max_jobs", ctypes.c_int32), ("tile", ctypes.c_int32),
-                ("pass_spp", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+                ("pass_spp", ctypes.c_int32), ("engine", ctypes.c_int32),
                 ("iteration_paths", ctypes.c_uint64), ("reserve_bytes", ctypes.c_uint64),
                 ("scene_cache_bytes", ctypes.c_uint64)]
 

@@ -138,4 +138,12 @@ cudaError_t serveLaunch(const ServeBatch& batch, int grid, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+cudaError_t serveFold(const ServeBatch& batch, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyToSymbolAsync(c_batch, &batch, sizeof batch, 0,
+                                          cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return e;
+  ptServeFold<<<batch.numItems, 256, 0, st>>>();
+  return cudaGetLastError();
+}
+
 }  // namespace sdb

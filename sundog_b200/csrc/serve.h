@@ -36,5 +36,7 @@ cudaError_t serveSetJob(int slot, const SdLaunch& lp, cudaStream_t st);
 int serveGridSize();
 // The batch's persistent render launch followed by its fold launch.
 cudaError_t serveLaunch(const ServeBatch& batch, int grid, cudaStream_t st);
+// The fold launch alone, for a batch rendered by the wavefront engine.
+cudaError_t serveFold(const ServeBatch& batch, cudaStream_t st);
 
 }  // namespace sdb

@@ -31,6 +31,7 @@
 #include "render_session.h"
 #include "scene_model.h"
 #include "serve.h"
+#include "wavefront.h"
 
 namespace sdb {
 
@@ -108,6 +109,11 @@ class Server {
     cudaCheck(cudaMallocHost((void**)&hItems, (size_t)maxItems * sizeof(ServeItem)), "pinned items");
     counters.alloc(2 * sizeof(unsigned long long));
     grid = serveGridSize();
+    if (cfg.engine != 1) {  // the wavefront engine's slot pool, sized for a batch
+      wf = wfAcquire();
+      uint64_t batchPaths = cfg.iteration_paths + (uint64_t)kMaxServeJobs * maxItemPaths;
+      wf->ensure((int)std::min<uint64_t>(batchPaths, 1ull << 26));
+    }
     slots.assign(kMaxServeJobs, nullptr);
     thread = std::thread([this] { loop(); });
   }
@@ -122,6 +128,7 @@ class Server {
     }
     cv.notify_all();
     if (thread.joinable()) thread.join();
+    wfRelease(std::move(wf));
     for (auto& j : slots)
       if (j) j->film.release();
     sceneCache.clear();
@@ -202,6 +209,7 @@ class Server {
   cudaStream_t st = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   DevBuf scratch, dItems, counters;
+  std::unique_ptr<WfBuffers> wf;  // engine 0: the wavefront engine's slot pool
   ServeItem* hItems = nullptr;
   int maxItems = 0;
   uint64_t maxItemPaths = 0;
@@ -346,6 +354,7 @@ class Server {
     j->lp.sampleOffset = 0;
     j->lp.sppThisLaunch = j->spp;
     cudaCheck(serveSetJob(slot, j->lp, st), "job table");
+    if (wf) cudaCheck(wfSetJob(slot, j->lp, st), "job table");
     j->slot = slot;
     slots[slot] = j;
     j->tilesX = (j->width + cfg.tile - 1) / cfg.tile;
@@ -475,7 +484,12 @@ class Server {
     b.rayCounter = (unsigned long long*)counters.ptr + 1;
     b.sampleL = (float4*)scratch.ptr;
     cudaCheck(cudaEventRecord(ev0, st), "event");
-    cudaCheck(serveLaunch(b, grid, st), "serve launch");
+    if (wf) {
+      wfRenderBatch(b, *wf, st);
+      cudaCheck(serveFold(b, st), "serve fold");
+    } else {
+      cudaCheck(serveLaunch(b, grid, st), "serve launch");
+    }
     cudaCheck(cudaEventRecord(ev1, st), "event");
     unsigned long long r = 0;
     cudaCheck(cudaMemcpyAsync(&r, b.rayCounter, sizeof r, cudaMemcpyDeviceToHost, st), "rays");
@@ -603,6 +617,7 @@ extern "C" sundog_server* sundog_server_create(const sundog_server_config* c) {
   if (cfg.tile < 8 || cfg.tile % 8 != 0 || cfg.tile > 1024)
     throw std::runtime_error("server: tile must be a multiple of 8 in 8..1024");
   if (cfg.pass_spp < 1) throw std::runtime_error("server: pass_spp must be positive");
+  if (cfg.engine < 0 || cfg.engine > 2) throw std::runtime_error("server: engine must be 0, 1 or 2");
   uint64_t itemPaths = (uint64_t)(cfg.tile / 8) * (cfg.tile / 8) * 64 * cfg.pass_spp;
   if (cfg.iteration_paths < itemPaths)
     throw std::runtime_error("server: iteration_paths is smaller than one tile-pass");

@@ -28,6 +28,7 @@
 #include <stdexcept>
 
 #include "pt_path.cuh"
+#include "serve.h"
 #include "wavefront.h"
 
 namespace sdb {
@@ -36,6 +37,21 @@ namespace cg = cooperative_groups;
 
 __constant__ SdLaunch c_wlp;
 __constant__ WfPool c_pool;
+
+// Serving batches (GUIDE & kWfServe): tile-passes of many jobs in one pool.
+// Each slot's path reads its job's launch block from this table (pool.jobs
+// holds the job slot); path ids map to tile-passes as in ptServe (serve.cu),
+// and finished samples go to the batch's sample buffer at their path id.
+constexpr int kWfServe = 4;
+__constant__ SdLaunch c_wjobs[kMaxServeJobs];
+__constant__ ServeBatch c_wbatch;
+
+// Launch block of the path in `slot`.
+template <int GUIDE>
+__device__ __forceinline__ const SdLaunch& slotLaunch(int slot) {
+  if (GUIDE & kWfServe) return c_wjobs[c_pool.jobs[slot]];
+  return c_wlp;
+}
 
 #ifndef SDB_WF_TRACE_BLOCKS
 #define SDB_WF_TRACE_BLOCKS 8
@@ -56,11 +72,36 @@ __device__ __forceinline__ unsigned appendSlot(unsigned* count) {
   return g.shfl(base, 0) + g.thread_rank();
 }
 
+template <int GUIDE>
 __device__ __forceinline__ unsigned long long nextPathId() {
   cg::coalesced_group g = cg::coalesced_threads();
+  unsigned long long* counter = (GUIDE & kWfServe) ? c_wbatch.pathCounter : c_wlp.pathCounter;
   unsigned long long base = 0;
-  if (g.thread_rank() == 0) base = atomicAdd(c_wlp.pathCounter, (unsigned long long)g.size());
+  if (g.thread_rank() == 0) base = atomicAdd(counter, (unsigned long long)g.size());
   return g.shfl(base, 0) + g.thread_rank();
+}
+
+// Serving: path id -> its tile-pass's camera sample (false for block
+// padding), as serveStart in serve.cu.
+__device__ __forceinline__ bool serveStartW(unsigned long long id, Path& p, int& job) {
+  const ServeBatch& b = c_wbatch;
+  int lo = 0, hi = b.numItems - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (b.items[mid].pathBegin <= id) lo = mid;
+    else hi = mid - 1;
+  }
+  const ServeItem& it = b.items[lo];
+  unsigned long long local = id - it.pathBegin;
+  int sLocal = (int)(local / (unsigned long long)it.npad);
+  int rem = (int)(local - (unsigned long long)sLocal * it.npad);
+  int blk = rem >> 6, within = rem & 63;
+  int lx = (blk % it.bw) * 8 + (within & 7), ly = (blk / it.bw) * 8 + (within >> 3);
+  if (lx >= it.w || ly >= it.h) return false;
+  job = it.job;
+  startPathAt(c_wjobs[job], it.x0 + lx, it.y0 + ly, it.sampleBegin + sLocal, p);
+  p.slot = (int)id;
+  return true;
 }
 
 // Puts the next camera path in `slot` and lists it in list `out`; leaves the
@@ -68,14 +109,16 @@ __device__ __forceinline__ unsigned long long nextPathId() {
 // kGuideRecord) start the slot's trail empty.
 template <int GUIDE>
 __device__ __forceinline__ void refill(int slot, int out) {
-  const SdLaunch& lp = c_wlp;
   const WfPool& pool = c_pool;
+  const unsigned long long numPaths = (GUIDE & kWfServe) ? c_wbatch.numPaths : c_wlp.numPaths;
   while (true) {
-    unsigned long long id = nextPathId();
-    if (id >= lp.numPaths) return;
+    unsigned long long id = nextPathId<GUIDE>();
+    if (id >= numPaths) return;
     Path p;
-    if (startPath(lp, id, p)) {
+    int job = 0;
+    if ((GUIDE & kWfServe) ? serveStartW(id, p, job) : startPath(c_wlp, id, p)) {
       pool.paths[slot].v = p;
+      if (GUIDE & kWfServe) pool.jobs[slot] = (unsigned char)job;
       if (GUIDE & kGuideRecord) pool.trails[slot].v.n = 0;
       pool.lists[out][appendSlot(&pool.counts[out])] = slot;
       return;
@@ -89,12 +132,15 @@ template <int GUIDE>
 __device__ __forceinline__ void finishPath(const Path& p, int slot) {
   float3 L = sanitize3(p.L);
   if (GUIDE & kGuideRecord) guideFlush(c_wlp, c_pool.trails[slot].v, L);
-  c_wlp.sampleL[p.slot] = make_float4(L.x, L.y, L.z, 1.0f);
+  float4* sampleL = (GUIDE & kWfServe) ? c_wbatch.sampleL : c_wlp.sampleL;
+  sampleL[p.slot] = make_float4(L.x, L.y, L.z, 1.0f);
 }
 
+template <int GUIDE = 0>
 __device__ __forceinline__ void addRays(unsigned long long rays) {
   for (int off = 16; off > 0; off >>= 1) rays += __shfl_down_sync(0xFFFFFFFFu, rays, off);
-  if ((threadIdx.x & 31) == 0 && rays) atomicAdd(c_wlp.rayCounter, rays);
+  unsigned long long* counter = (GUIDE & kWfServe) ? c_wbatch.rayCounter : c_wlp.rayCounter;
+  if ((threadIdx.x & 31) == 0 && rays) atomicAdd(counter, rays);
 }
 
 template <int GUIDE>
@@ -284,14 +330,35 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
   addRays(rays);
 }
 
-template <int GUIDE>
-__global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeA(int in, int out) {
-  const SdLaunch& lp = c_wlp;
+// Serving batches: the radiance rays of the live list, each traversing its
+// own job's scene (traverse<false> of sd_trace.cuh, grid-stride).
+__global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceServe(int in) {
   const WfPool& pool = c_pool;
   const unsigned n = pool.counts[in];
   unsigned long long rays = 0;
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int slot = pool.lists[in][i];
+    const SdLaunch& lp = slotLaunch<kWfServe>(slot);
+    const Path& p = pool.paths[slot].v;
+    TraceHit h;
+    float dummyTr = 1.0f;
+    float3 dummyTau = v3(0.0f);
+    bool hit = traverse<false, false>(lp, p.o, p.d, 1e16f, h, dummyTr, dummyTau, nullptr);
+    if (!hit) h.inst = -1;
+    pool.hits[slot].v = h;
+    rays++;
+  }
+  addRays<kWfServe>(rays);
+}
+
+template <int GUIDE>
+__global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeA(int in, int out) {
+  const WfPool& pool = c_pool;
+  const unsigned n = pool.counts[in];
+  unsigned long long rays = 0;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int slot = pool.lists[in][i];
+    const SdLaunch& lp = slotLaunch<GUIDE>(slot);
     Path p = pool.paths[slot].v;
     TraceHit h = pool.hits[slot].v;
     Vertex v;
@@ -306,15 +373,16 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeA(in
       refill<GUIDE>(slot, out);
     }
   }
-  addRays(rays);
+  addRays<GUIDE>(rays);
 }
 
+template <int GUIDE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfShadow() {
-  const SdLaunch& lp = c_wlp;
   const WfPool& pool = c_pool;
   const unsigned n = pool.counts[2];
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int slot = pool.shadowList[i];
+    const SdLaunch& lp = slotLaunch<GUIDE>(slot);
     const Vertex& v = pool.verts[slot].v;
     float3 tr = shadowTransmittance<false>(lp, v.so, v.wi, v.tmaxS, nullptr);
     pool.trs[slot] = make_float4(tr.x, tr.y, tr.z, 0.0f);
@@ -326,12 +394,12 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfShadow() 
 // kGuideRecord: the guided vertex joins the slot's trail.
 template <int GUIDE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeB(int in, int out) {
-  const SdLaunch& lp = c_wlp;
   const WfPool& pool = c_pool;
   const unsigned n = pool.counts[in];
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int slot = pool.lists[in][i];
     if (!pool.pending[slot]) continue;
+    const SdLaunch& lp = slotLaunch<GUIDE>(slot);
     Path p = pool.paths[slot].v;
     const Vertex v = pool.verts[slot].v;
     float3 tr = v3(0.0f);
@@ -380,12 +448,13 @@ void WfBuffers::ensure(int slots) {
   list0.alloc((size_t)slots * sizeof(int));
   list1.alloc((size_t)slots * sizeof(int));
   shadow.alloc((size_t)slots * sizeof(int));
+  jobs.alloc((size_t)slots);
   if (!counts.ptr) counts.alloc(4 * sizeof(unsigned));
   if (!hostCount) cudaCheck(cudaMallocHost((void**)&hostCount, sizeof(unsigned)), "pinned count");
   cap = slots;
   gridTrace = gridFor(wfTraceFetch);
   gridShadeA = gridFor(wfShadeA<0>);
-  gridShadow = gridFor(wfShadow);
+  gridShadow = gridFor(wfShadow<0>);
   gridShadeB = gridFor(wfShadeB<0>);
   gridStart = gridFor(wfStart<0>);
 }
@@ -424,24 +493,27 @@ void wfRelease(std::unique_ptr<WfBuffers> b) {
 
 size_t wfSlotBytes() {
   return sizeof(PoolSlot<Path>) + sizeof(PoolSlot<Vertex>) + sizeof(PoolSlot<TraceHit>) +
-         sizeof(float4) + 1 + 3 * sizeof(int);
+         sizeof(float4) + 2 + 3 * sizeof(int);
 }
 
 // Renders the launch block's paths (lp.numPaths ids, counters already
 // cleared) into lp.sampleL through the stages. Returns the kernels launched.
-// One iteration's stage kernels for guide mode GUIDE.
+// One iteration's stage kernels for mode GUIDE (guide bits, or kWfServe).
 template <int GUIDE>
 static void wfIteration(const WfBuffers& b, cudaStream_t st, int cur, int nxt) {
-  wfTraceFetch<<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
+  if (GUIDE & kWfServe)
+    wfTraceServe<<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
+  else
+    wfTraceFetch<<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
   wfShadeA<GUIDE><<<b.gridShadeA, kRenderBlock, 0, st>>>(cur, nxt);
-  wfShadow<<<b.gridShadow, kRenderBlock, 0, st>>>();
+  wfShadow<GUIDE><<<b.gridShadow, kRenderBlock, 0, st>>>();
   wfShadeB<GUIDE><<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
 }
 
-int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
-  if (guide < 0 || guide > (kGuideSample | kGuideRecord))
-    throw std::runtime_error("wavefront: invalid guide mode");
-  if (guide & kGuideRecord) b.ensureTrails();
+// Fills the pool with the first paths of ids [0, numPaths) and runs stage
+// iterations until no path is live (the launch block or batch is already in
+// constant memory). Returns the kernels launched.
+static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, int mode) {
   WfPool pool;
   pool.paths = (PoolSlot<Path>*)b.paths.ptr;
   pool.verts = (PoolSlot<Vertex>*)b.verts.ptr;
@@ -453,14 +525,15 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
   pool.shadowList = (int*)b.shadow.ptr;
   pool.counts = (unsigned*)b.counts.ptr;
   pool.trails = (PoolSlot<GuideTrail>*)b.trails.ptr;
-  pool.cap = (int)std::min<unsigned long long>((unsigned long long)b.cap, lp.numPaths);
-  cudaCheck(cudaMemcpyToSymbolAsync(c_wlp, &lp, sizeof lp, 0, cudaMemcpyHostToDevice, st),
-            "wavefront launch block");
+  pool.jobs = (unsigned char*)b.jobs.ptr;
+  pool.cap = (int)std::min<unsigned long long>((unsigned long long)b.cap, numPaths);
   cudaCheck(cudaMemcpyToSymbolAsync(c_pool, &pool, sizeof pool, 0, cudaMemcpyHostToDevice, st),
             "wavefront pool");
   cudaCheck(cudaMemsetAsync(b.counts.ptr, 0, b.counts.bytes, st), "wavefront counts");
   int launches = 0;
-  if (guide & kGuideRecord)
+  if (mode & kWfServe)
+    wfStart<kWfServe><<<b.gridStart, kRenderBlock, 0, st>>>();
+  else if (mode & kGuideRecord)
     wfStart<kGuideRecord><<<b.gridStart, kRenderBlock, 0, st>>>();
   else
     wfStart<0><<<b.gridStart, kRenderBlock, 0, st>>>();
@@ -472,11 +545,12 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
     int nxt = 1 - cur;
     cudaCheck(cudaMemsetAsync(counts + nxt, 0, sizeof(unsigned), st), "wavefront counts");
     cudaCheck(cudaMemsetAsync(counts + 2, 0, 2 * sizeof(unsigned), st), "wavefront counts");
-    switch (guide) {
+    switch (mode) {
       case 0: wfIteration<0>(b, st, cur, nxt); break;
       case kGuideSample: wfIteration<kGuideSample>(b, st, cur, nxt); break;
       case kGuideRecord: wfIteration<kGuideRecord>(b, st, cur, nxt); break;
-      default: wfIteration<kGuideSample | kGuideRecord>(b, st, cur, nxt); break;
+      case kGuideSample | kGuideRecord: wfIteration<kGuideSample | kGuideRecord>(b, st, cur, nxt); break;
+      default: wfIteration<kWfServe>(b, st, cur, nxt); break;
     }
     cudaCheck(cudaGetLastError(), "wavefront stage");
     launches += 4;
@@ -489,6 +563,27 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
     if (iter > (1 << 24)) throw std::runtime_error("wavefront: no progress");
   }
   return launches;
+}
+
+int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
+  if (guide < 0 || guide > (kGuideSample | kGuideRecord))
+    throw std::runtime_error("wavefront: invalid guide mode");
+  if (guide & kGuideRecord) b.ensureTrails();
+  cudaCheck(cudaMemcpyToSymbolAsync(c_wlp, &lp, sizeof lp, 0, cudaMemcpyHostToDevice, st),
+            "wavefront launch block");
+  return runPool(b, st, lp.numPaths, guide);
+}
+
+cudaError_t wfSetJob(int slot, const SdLaunch& lp, cudaStream_t st) {
+  if (slot < 0 || slot >= kMaxServeJobs) return cudaErrorInvalidValue;
+  return cudaMemcpyToSymbolAsync(c_wjobs, &lp, sizeof(SdLaunch), slot * sizeof(SdLaunch),
+                                 cudaMemcpyHostToDevice, st);
+}
+
+int wfRenderBatch(const ServeBatch& batch, WfBuffers& b, cudaStream_t st) {
+  cudaCheck(cudaMemcpyToSymbolAsync(c_wbatch, &batch, sizeof batch, 0, cudaMemcpyHostToDevice, st),
+            "wavefront batch");
+  return runPool(b, st, batch.numPaths, kWfServe);
 }
 
 }  // namespace sdb

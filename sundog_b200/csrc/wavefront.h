@@ -37,12 +37,13 @@ struct WfPool {
   unsigned* counts;        // [0], [1]: list lengths; [2]: shadow-list length;
                            // [3]: rays the trace stage has fetched
   PoolSlot<GuideTrail>* trails;  // guided vertices awaiting their path's end (record passes)
+  unsigned char* jobs;     // serving batches: the job slot of each slot's path
   int cap;
 };
 
 // Host-owned pool storage, grown on demand.
 struct WfBuffers {
-  DevBuf paths, verts, hits, trs, pending, list0, list1, shadow, counts;
+  DevBuf paths, verts, hits, trs, pending, list0, list1, shadow, counts, jobs;
   DevBuf trails;  // allocated by the first training-record pass
   unsigned* hostCount = nullptr;
   int cap = 0;
@@ -69,5 +70,12 @@ void wfRelease(std::unique_ptr<WfBuffers> b);
 // kGuideRecord (keep each path's guided vertices in its slot's trail and turn
 // them into training records when the path ends).
 int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide = 0);
+
+// Serving batches (serve.h): job slot `slot` of the engine's job table, and
+// one batch of tile-passes rendered through the pool into batch.sampleL at
+// each path's id (the caller folds them). Returns the kernels launched.
+struct ServeBatch;
+cudaError_t wfSetJob(int slot, const SdLaunch& lp, cudaStream_t st);
+int wfRenderBatch(const ServeBatch& batch, WfBuffers& b, cudaStream_t st);
 
 }  // namespace sdb

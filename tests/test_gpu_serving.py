@@ -1,9 +1,13 @@
 """The render server (sundog_server_*): continuous batching of tile-passes
 from several jobs in one persistent launch.
 
-  * every job's film is bit-identical to a session render of the same
-    scene, size, spp and seed with the persistent megakernel -- alone on the server and mixed with other
-    scenes' jobs (ragged edge tiles, spp not a multiple of the pass size);
+  * every job's film is the same, bit for bit, alone on the server and
+    mixed with other scenes' jobs (ragged edge tiles, spp not a multiple of
+    the pass size); with the megakernel engine it is bit-identical to a
+    session render of the same scene, size, spp and seed with the megakernel,
+    and with the wavefront engine (the default) it equals the wavefront
+    session render up to FP32 rounding (the same per-path code compiled into
+    other kernels: compared as the engines are in test_gpu_render.py);
   * host-side failures end only the affected job: a missing asset (FAILED
     with the loader's message), a film larger than the device (FAILED, not
     admitted), cancellation of queued and running jobs;
@@ -23,11 +27,19 @@ from sundog_b200.scene import scale
 pytestmark = pytest.mark.gpu
 
 
-def session_film(s, base_dir, **opts):
-    # The server runs the persistent megakernel's path code (engine 1).
-    with sc.Session(s, base_dir=base_dir, engine=1, **opts) as ses:
+def session_film(s, base_dir, engine=1, **opts):
+    with sc.Session(s, base_dir=base_dir, engine=engine, **opts) as ses:
         ses.render()
         return ses.read()
+
+
+def close_films(a, b):
+    """Films of the same samples from differently compiled kernels: FP32
+    rounding, amplified only where a path's decision flips."""
+    a = a[..., :3].astype(np.float64)
+    b = b[..., :3].astype(np.float64)
+    err = np.abs(a - b) / np.maximum(np.abs(b), 1e-3)
+    return np.quantile(err, 0.99) <= 1e-4 and np.abs(a.mean() - b.mean()) <= 1e-3 * abs(b.mean())
 
 
 def mix(asset_dir):
@@ -39,22 +51,28 @@ def mix(asset_dir):
     ]
 
 
-def test_jobs_equal_alone_and_mixed(lib, asset_dir):
+@pytest.mark.parametrize("engine", [0, 1])
+def test_jobs_equal_alone_and_mixed(lib, asset_dir, engine):
     jobs = mix(asset_dir)
-    refs = [session_film(s, asset_dir, **o) for s, o in jobs]
-    cfg = dict(tile=32, pass_spp=4, iteration_paths=1 << 16)
+    refs = [session_film(s, asset_dir, engine=engine, **o) for s, o in jobs]
+    cfg = dict(tile=32, pass_spp=4, iteration_paths=1 << 16, engine=engine)
     # Alone: one job per server.
+    alone = []
     for (s, o), ref in zip(jobs, refs):
         with serve.Server(**cfg) as sv:
             film = sv.submit(s, base_dir=asset_dir, **o).wait()
-            assert np.array_equal(film, ref)
+            alone.append(film)
+            if engine == 1:
+                assert np.array_equal(film, ref)
+            else:
+                assert close_films(film, ref)
     # Mixed: all jobs in flight together.
     with serve.Server(**cfg) as sv:
         handles = [sv.submit(s, base_dir=asset_dir, **o) for s, o in jobs]
         films = [h.wait() for h in handles]
         st = sv.stats()
-    for f, ref in zip(films, refs):
-        assert np.array_equal(f, ref)
+    for f, a in zip(films, alone):
+        assert np.array_equal(f, a)
     assert st.jobs_done == len(jobs) and st.jobs_failed == 0
     assert st.paths == sum(o["width"] * o["height"] * o["spp"] for _, o in jobs)
     assert st.rays > st.paths and st.iterations > 1
@@ -75,8 +93,8 @@ def test_missing_asset_fails_only_that_job(lib, asset_dir, tmp_path):
         with pytest.raises(serve.JobError, match="does_not_exist.obj"):
             jb.wait()
         assert jb.last.state == abi.JOB_FAILED
-        ref = session_film(good, ".", width=48, height=48, spp=2)
-        assert np.array_equal(jg.wait(), ref)
+        ref = session_film(good, ".", engine=0, width=48, height=48, spp=2)
+        assert close_films(jg.wait(), ref)
 
 
 def test_oversized_job_is_refused(lib):
