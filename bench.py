@@ -77,6 +77,10 @@ def parse_args():
                     help="render-server line (Poisson jobs, p50/p99 latency) instead of Mrays/s")
     ap.add_argument("--serve-jobs", type=int, default=60)
     ap.add_argument("--serve-rate", type=float, default=20.0)
+    ap.add_argument("--serve-batch", type=int, default=0,
+                    help="camera paths per server batch (0 = the server's default)")
+    ap.add_argument("--serve-engine", type=int, default=0, choices=[0, 1, 2],
+                    help="server kernels: 0 wavefront, 1 megakernel")
     return ap.parse_args()
 
 
@@ -573,12 +577,15 @@ def run_serving(args):
     work = [(int(k), int(w), int(p)) for k, w, p in zip(kinds, sides, spps)]
     # Warm-up: every scene once (module load, scene builds), then a fresh
     # server for the timed run so no scene is resident when it starts.
-    with serve.Server() as sv:
+    cfg = {"engine": args.serve_engine}
+    if args.serve_batch > 0:
+        cfg["iteration_paths"] = args.serve_batch
+    with serve.Server(**cfg) as sv:
         for s in scenes:
             sv.submit(s, base_dir=ad, width=64, height=64, spp=1, film=False).wait()
     sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     sampler.start()
-    with serve.Server() as sv:
+    with serve.Server(**cfg) as sv:
         t0 = time.perf_counter()
         jobs = []
         for (k, side, spp), at in zip(work, arrivals):
@@ -609,7 +616,8 @@ def run_serving(args):
                                "tile-passes of 8 spp batched across jobs",
                    "jobs": n, "arrival_rate_per_s": args.serve_rate,
                    "max_jobs": sv.config.max_jobs,
-                   "iteration_paths": sv.config.iteration_paths},
+                   "iteration_paths": sv.config.iteration_paths,
+                   "engine": ["wavefront", "megakernel", "wavefront"][sv.config.engine]},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "mean": float(np.mean(lat)), "max": float(np.max(lat))},
         "queued_ms": {"p50": float(np.percentile(queued, 50)),
