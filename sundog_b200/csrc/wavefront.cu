@@ -166,14 +166,16 @@ __global__ void __launch_bounds__(kRenderBlock) wfStart() {
 // live list (one warp-aggregated atomicAdd on counts[3]), so a warp no longer
 // waits for its longest ray. Each ray visits the nodes of traverse<false>
 // (sd_trace.cuh) in the same order with the same tests: the same closest
-// accepted hit. (Shadow rays, shorter, gained nothing from it.)
+// accepted hit. (Shadow rays, shorter, gained nothing from it.) SERVE: a
+// serving batch, each lane tracing in its own job's scene.
+template <bool SERVE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetch(int in) {
-  const SdLaunch& lp = c_wlp;
   const WfPool& pool = c_pool;
   const unsigned n = pool.counts[in];
   const unsigned full = 0xFFFFFFFFu;
   const unsigned ltMask = (1u << (threadIdx.x & 31)) - 1u;
-  const BvhNode* nodes = lp.nodes;
+  const BvhNode* nodes = c_wlp.nodes;
+  int job = 0;  // SERVE: the lane's job slot
   const float tmin = 0.0f;
   unsigned long long rays = 0;
   int slot = -1;
@@ -197,6 +199,8 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
         unsigned i = base + __popc(idle & ltMask);
         if (i < n) {
           slot = pool.lists[in][i];
+          if (SERVE) job = pool.jobs[slot];
+          const SdLaunch& jl = SERVE ? c_wjobs[job] : c_wlp;
           O = pool.paths[slot].v.o;
           D = pool.paths[slot].v.d;
           ro = O;
@@ -208,7 +212,7 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
           inBlas = false;
           curInst = -1;
           sp = 0;
-          cur = lp.numInstances > 0 ? lp.tlasRoot : kPop;
+          cur = jl.numInstances > 0 ? jl.tlasRoot : kPop;
         }
       }
     }
@@ -217,8 +221,9 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
       continue;
     }
     if (slot < 0) continue;
+    const SdLaunch& lp = SERVE ? c_wjobs[job] : c_wlp;
     if (cur >= 0) {
-      BvhNode nd = loadNode(nodes, cur);
+      BvhNode nd = loadNode(SERVE ? lp.nodes : nodes, cur);
       float ta, tb;
       bool ha, hb;
       boxPair(nd, oi, id, tmin, tmax, ta, tb, ha, hb);
@@ -327,28 +332,7 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
       hit.front = front;
     }
   }
-  addRays(rays);
-}
-
-// Serving batches: the radiance rays of the live list, each traversing its
-// own job's scene (traverse<false> of sd_trace.cuh, grid-stride).
-__global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceServe(int in) {
-  const WfPool& pool = c_pool;
-  const unsigned n = pool.counts[in];
-  unsigned long long rays = 0;
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int slot = pool.lists[in][i];
-    const SdLaunch& lp = slotLaunch<kWfServe>(slot);
-    const Path& p = pool.paths[slot].v;
-    TraceHit h;
-    float dummyTr = 1.0f;
-    float3 dummyTau = v3(0.0f);
-    bool hit = traverse<false, false>(lp, p.o, p.d, 1e16f, h, dummyTr, dummyTau, nullptr);
-    if (!hit) h.inst = -1;
-    pool.hits[slot].v = h;
-    rays++;
-  }
-  addRays<kWfServe>(rays);
+  addRays<SERVE ? kWfServe : 0>(rays);
 }
 
 template <int GUIDE>
@@ -452,7 +436,7 @@ void WfBuffers::ensure(int slots) {
   if (!counts.ptr) counts.alloc(4 * sizeof(unsigned));
   if (!hostCount) cudaCheck(cudaMallocHost((void**)&hostCount, sizeof(unsigned)), "pinned count");
   cap = slots;
-  gridTrace = gridFor(wfTraceFetch);
+  gridTrace = gridFor(wfTraceFetch<false>);
   gridShadeA = gridFor(wfShadeA<0>);
   gridShadow = gridFor(wfShadow<0>);
   gridShadeB = gridFor(wfShadeB<0>);
@@ -501,10 +485,7 @@ size_t wfSlotBytes() {
 // One iteration's stage kernels for mode GUIDE (guide bits, or kWfServe).
 template <int GUIDE>
 static void wfIteration(const WfBuffers& b, cudaStream_t st, int cur, int nxt) {
-  if (GUIDE & kWfServe)
-    wfTraceServe<<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
-  else
-    wfTraceFetch<<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
+  wfTraceFetch<(GUIDE & kWfServe) != 0><<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
   wfShadeA<GUIDE><<<b.gridShadeA, kRenderBlock, 0, st>>>(cur, nxt);
   wfShadow<GUIDE><<<b.gridShadow, kRenderBlock, 0, st>>>();
   wfShadeB<GUIDE><<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
