@@ -189,7 +189,8 @@ typedef struct {
   float* film_rgba;
   float* aov_albedo;
   float* aov_normal;
-  int32_t chunk_spp;     /* samples per persistent launch; <= 0 = automatic */
+  int32_t chunk_spp;     /* samples per chunk (one persistent launch, or one
+                            pass of the wavefront engine); <= 0 = automatic */
   int32_t repeat;        /* >1: re-render the film this many times and report
                             the fastest render loop (timing aid); 0/1 = once */
   int32_t guiding;       /* 1 = learned path guiding (see sundog_guiding_*) */
@@ -382,9 +383,9 @@ SUNDOG_API int sundog_guide_gradients(const float* params, const float* records,
  * device memory are available (jobs that fit pass one that does not), keeps
  * each scene's device data (BVH, CDFs, textures, meshes) resident and shared
  * by all jobs of that scene, and renders all admitted jobs together: each
- * iteration is one persistent launch over tile-passes (a tile x tile pixel
- * rectangle and a range of its samples) drawn from every active job, then one
- * fold of those samples into each job's film. Jobs arriving while others run
+ * iteration renders one batch of tile-passes (a tile x tile pixel rectangle
+ * and a range of its samples) drawn from every active job, then folds those
+ * samples into each job's film. Jobs arriving while others run
  * join at the next iteration. A job's film is the same alone or in any mix
  * of jobs, bit for bit; with engine 1 it is bit-identical to a
  * sundog_session_render of the same scene, size, spp and seed with the
@@ -422,7 +423,7 @@ typedef struct {
 
 typedef struct {
   uint64_t jobs_submitted, jobs_done, jobs_failed, jobs_cancelled;
-  uint64_t iterations;         /* persistent launches */
+  uint64_t iterations;         /* batches rendered */
   uint64_t rays;               /* radiance + shadow traces of all jobs */
   uint64_t paths;              /* camera paths of all jobs */
   double busy_ms;              /* CUDA-event time of the iterations */
