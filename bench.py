@@ -185,13 +185,9 @@ def bytes_per_ray(c):
 def oracle_sample(scene, base_dir, args, seconds, threads):
     """Render a band of rows of the same frame with the CPU oracle."""
     from oracle import oracle
-    from sundog_b200 import scene as sc
-    h = scene.build(base_dir)
-    try:
-        state = sc.debug_json(h)
-    finally:
-        sc.abi.load().sundog_scene_destroy(h)
-    text, r = oracle.scene_text(state, base_dir)
+    # The scene as sundog's own scene code derives it (oracle/_ref), so the
+    # CPU arm loads nothing of this library.
+    text, r = oracle.reference_scene_text(scene, base_dir)
     osc = oracle.OracleScene(text)
     W, H, spp = r["width"], r["height"], r["spp"]
     # calibrate on one row

@@ -278,20 +278,22 @@ SUNDOG_API int sundog_session_trace_counts(sundog_session*, sundog_trace_counts*
 
 /* Allocation-free tile render (no counterpart in the reference). For callers
  * that cannot allocate device memory when they render, such as a serving
- * worker whose device memory is owned by another allocator, or code being
- * recorded into a CUDA graph: renders samples [sample_begin, sample_begin +
- * sample_count) of the pixel rectangle (x0, y0, w, h) of a resident session's
- * image and folds them in sample order into film_device, w*h float4 running
- * means in device memory the caller owns (zeros for sample_begin 0). The
- * pixels equal the same pixels of a full render of the session. Calls no
- * cudaMalloc/cudaFree: its scratch is a static 16 MiB device array in the
- * library (held by every GPU that loads it until exit), so w*h*sample_count
- * may not exceed 1048576 (64x64 at 256 spp); larger requests fail. All calls
- * share that array: calls that overlap on the GPU race, serialise them. The
- * first call on a device looks the array up and should precede any stream
- * capture. rays_out (host, may be NULL): radiance + shadow traces; when
- * given, the call waits for completion. cuda_stream NULL = default stream.
- * Returns 0/1. */
+ * worker whose device memory is owned by another allocator or held to a fixed
+ * budget: renders samples [sample_begin, sample_begin + sample_count) of the
+ * pixel rectangle (x0, y0, w, h) of a resident session's image and folds them
+ * in sample order into film_device, w*h float4 running means in device memory
+ * the caller owns (zeros for sample_begin 0). Sample indices count from the
+ * session's first sample (its sample_offset), so the pixels equal the same
+ * pixels of a full render of the session. Sessions with learned guiding
+ * enabled are rejected (plain samples only). Calls no cudaMalloc/cudaFree:
+ * its scratch is a static 16 MiB device array in the library (held by every
+ * GPU that loads it until exit), so w*h*sample_count may not exceed 1048576
+ * (64x64 at 256 spp); larger requests fail. All calls share that array and it
+ * keeps the last call's contents: calls that overlap on the GPU race,
+ * serialise them. The first call on a device looks the array up (with that
+ * device current) and should come before any stream capture. rays_out (host,
+ * may be NULL): radiance + shadow traces; when given, the call waits for
+ * completion. cuda_stream NULL = default stream. Returns 0/1. */
 SUNDOG_API int sundog_session_render_tile_noalloc(sundog_session*, int x0, int y0, int w, int h,
                                                   int sample_begin, int sample_count,
                                                   float* film_device, uint64_t* rays_out,

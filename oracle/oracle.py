@@ -1,10 +1,17 @@
 """ORACLE — test infrastructure only (the checker, never the product).
 
 Python front end of the CPU oracle (oracle/_build/libsdoracle.so, built by
-oracle/Makefile). It turns a scene's parse-time state (the JSON the library
-reports through sundog_scene_debug_json) into the oracle's text description,
-loads it, and renders pixel rectangles on the host cores. It also exposes the
-oracle's function harness (sdo_fn) for per-function parity checks.
+oracle/Makefile). The oracle's scene comes from the reference itself:
+reference_scene_text() replays a scene's calls into sundog's own
+scene-construction code (src/capi_scene.cpp + src/scene_build.cpp, compiled
+into oracle/_ref/libsdref_scene.so by `make ref`), which derives the camera
+settings, transforms, NEE light registration and flame lights, and writes the
+result as the oracle's text description. The oracle loads that and renders
+pixel rectangles on the host cores. scene_text() turns a library's
+parse-time state (sundog_scene_debug_json) into the same description; the
+tests use it only to compare the product's derivation with the reference's.
+The module also exposes the oracle's function harness (sdo_fn) for
+per-function parity checks.
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use it.
 """
@@ -17,21 +24,100 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libsdoracle.so")
 REF_FNVEC = os.path.join(HERE, "_ref", "fnvec_ref")
+REF_SCENE_LIB = os.path.join(HERE, "_ref", "libsdref_scene.so")
 
 _lib = None
+_ref_scene = None
 
 
 def build(force=False):
-    """Compile the oracle with its Makefile (and the reference harness when
-    the reference sources are mounted)."""
+    """Compile the oracle with its Makefile, and the reference-built parts
+    (function harness, scene library) when the reference sources are
+    mounted."""
     import subprocess
+    from oracle.refpath import reference_root
     targets = ["all"]
-    if os.path.isdir("/root/reference/device"):
-        targets.append("ref")
+    ref = reference_root()
+    if ref is not None:
+        targets += ["ref", "REF=" + ref]
     if force:
         subprocess.run(["make", "-C", HERE, "clean"], check=True, stdout=subprocess.DEVNULL)
     subprocess.run(["make", "-C", HERE] + targets, check=True, stdout=subprocess.DEVNULL)
     return LIB_PATH
+
+
+def ref_scene_lib():
+    """sundog's own scene-construction library (oracle/_ref/libsdref_scene.so)
+    with the scene ABI's prototypes declared. Raises when it was never built:
+    it is built from the reference sources, which must be mounted once (the
+    built library then travels with the repository)."""
+    global _ref_scene
+    if _ref_scene is None:
+        if not os.path.isfile(REF_SCENE_LIB):
+            build()
+        if not os.path.isfile(REF_SCENE_LIB):
+            raise RuntimeError("oracle: %s is not built (it compiles sundog's own "
+                               "src/capi_scene.cpp and src/scene_build.cpp; mount the reference "
+                               "and run oracle.build())" % REF_SCENE_LIB)
+        from sundog_b200 import abi
+        lib = ctypes.CDLL(REF_SCENE_LIB, mode=ctypes.RTLD_LOCAL)
+        abi.declare_scene_abi(lib)
+        lib.sdo_ref_scene_text.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t,
+                                           ctypes.POINTER(ctypes.c_size_t)]
+        lib.sdo_ref_scene_forget.argtypes = [ctypes.c_void_p]
+        lib.sdo_ref_scene_forget.restype = None
+        _ref_scene = lib
+    return _ref_scene
+
+
+def apply_overrides(text, width=None, height=None, spp=None, seed=None, clamp=None,
+                    transparent_shadows=None):
+    """Applies sundog_render_options' overrides (src/capi_render.cpp:74-83:
+    spp / width / height when > 0, seed when >= 0, clamp when set and >= 0,
+    transparent shadows when >= 0) to the render line of an oracle
+    description. Returns (text, render dict)."""
+    lines = text.split("\n")
+    f = lines[0].split()
+    assert f[0] == "render", "oracle description must start with its render line"
+    r = {"width": int(f[1]), "height": int(f[2]), "spp": int(f[3]), "max_depth": int(f[4]),
+         "clamp": float(f[5]), "seed": int(f[6]), "transparent_shadows": int(f[7])}
+    if width:
+        r["width"] = width
+    if height:
+        r["height"] = height
+    if spp:
+        r["spp"] = spp
+    if seed is not None and seed >= 0:
+        r["seed"] = seed
+    if clamp is not None and clamp >= 0:
+        r["clamp"] = clamp
+    if transparent_shadows is not None and transparent_shadows >= 0:
+        r["transparent_shadows"] = transparent_shadows
+    lines[0] = "render %d %d %d %d %s %d %d" % (r["width"], r["height"], r["spp"],
+                                                 r["max_depth"], _f(r["clamp"]), r["seed"],
+                                                 r["transparent_shadows"])
+    return "\n".join(lines), r
+
+
+def reference_scene_text(scene, base_dir, **overrides):
+    """The oracle description of `scene` (a sundog_b200.scene.Scene: the
+    scenelib-style call list) as sundog's own scene code derives it: the
+    calls are replayed, in scenelib's order, into oracle/_ref/libsdref_scene.so
+    and the derived sd::Scene is written out. Returns (text, render dict)
+    with the render-option overrides applied."""
+    lib = ref_scene_lib()
+    h = scene.build(base_dir, lib)
+    try:
+        need = ctypes.c_size_t(0)
+        if lib.sdo_ref_scene_text(h, None, 0, ctypes.byref(need)) != 0:
+            raise RuntimeError("oracle: reference scene text failed")
+        buf = ctypes.create_string_buffer(need.value)
+        lib.sdo_ref_scene_text(h, buf, need.value, ctypes.byref(need))
+        text = buf.value.decode()
+    finally:
+        lib.sdo_ref_scene_forget(h)
+        lib.sundog_scene_destroy(h)
+    return apply_overrides(text, **overrides)
 
 
 def load():

@@ -162,15 +162,11 @@ ADDITIVE_SYMBOLS = [
 _lib = None
 
 
-def load(path=None):
-    """Load libsundog.so once and declare every prototype."""
-    global _lib
-    if _lib is not None and path is None:
-        return _lib
-    p = path or LIB_PATH
-    if not os.path.isfile(p):
-        raise RuntimeError("libsundog.so not built at %s (run sundog_b200.build.build())" % p)
-    lib = ctypes.CDLL(p, mode=ctypes.RTLD_GLOBAL)
+def declare_scene_abi(lib):
+    """Prototypes of the scene-construction half of the ABI (sundog_last_error
+    ... sundog_scene_validate, plus sundog_set_flame_steps) on a loaded
+    library. The CPU oracle applies them to its build of the reference's own
+    scene code, which exports the same functions."""
     vp, ip, dp, cp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_char_p
     d3 = ctypes.POINTER(ctypes.c_double)
     lib.sundog_last_error.restype = cp
@@ -201,9 +197,23 @@ def load(path=None):
     lib.sundog_add_point_light.argtypes = [vp, d3, d3, dp]
     lib.sundog_add_distant_light.argtypes = [vp, d3, d3]
     lib.sundog_scene_validate.argtypes = [vp]
+    lib.sundog_set_flame_steps.argtypes = [vp, ip, ip]
+    return lib
+
+
+def load(path=None):
+    """Load libsundog.so once and declare every prototype."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.isfile(p):
+        raise RuntimeError("libsundog.so not built at %s (run sundog_b200.build.build())" % p)
+    lib = ctypes.CDLL(p, mode=ctypes.RTLD_GLOBAL)
+    declare_scene_abi(lib)
+    vp, ip, dp, cp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_char_p
     lib.sundog_probe.argtypes = [ctypes.POINTER(DeviceInfo)]
     lib.sundog_render.argtypes = [vp, ctypes.POINTER(RenderOptions)]
-    lib.sundog_set_flame_steps.argtypes = [vp, ip, ip]
     lib.sundog_render_ex.argtypes = [vp, ctypes.POINTER(RenderOptions),
                                      ctypes.POINTER(RenderExt), ctypes.POINTER(RenderResult)]
     lib.sundog_scene_debug_json.argtypes = [vp, cp, ctypes.c_size_t,

@@ -1,9 +1,9 @@
 // Binned SAH build (Wald, "On fast Construction of SAH-based Bounding Volume
 // Hierarchies", 2007): 32 bins per axis over centroid bounds, all three axes
 // binned in one pass, ranges of up to 32 primitives split exactly over their
-// sorted centroids, leaf when splitting costs more than intersecting; below the
-// depth limit of 48 a median split guarantees termination, so a traversal
-// stack of 64 entries covers TLAS + BLAS depth.
+// sorted centroids, leaf when splitting costs more than intersecting; from the
+// depth limit of 40 on, median splits guarantee termination. The scene build
+// checks TLAS + BLAS depth against the traversal stack (kTraversalStack).
 #include "bvh_build.h"
 
 #include <algorithm>

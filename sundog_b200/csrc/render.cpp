@@ -390,6 +390,14 @@ void DeviceScene::build(const SceneDesc& desc) {
       allTris.push_back(make_float4(c.x, c.y, c.z, 0.0f));
     }
   }
+  // A traversal keeps at most one stack entry per tree level (plus its
+  // BLAS-entry entries), so trees this deep could fill the stack; reject them
+  // rather than let a ray skip part of the scene.
+  const int depthRoom = wide ? kCwTraversalStack - 4 : kTraversalStack - 2;
+  if (tlasDepth + blasDepth > depthRoom)
+    throw std::runtime_error("scene: BVH too deep for the traversal stack (TLAS depth " +
+                             std::to_string(tlasDepth) + " + BLAS depth " +
+                             std::to_string(blasDepth) + " > " + std::to_string(depthRoom) + ")");
   // Instances in TLAS leaf order (leaf primitive index = position here).
   std::vector<SdInstance> inst(nObj);
   for (int k = 0; k < nObj; k++) {

@@ -28,7 +28,7 @@
 
 namespace sdb {
 
-constexpr int kStackSize = 64;
+constexpr int kStackSize = kTraversalStack;
 constexpr int kPop = (int)0x80000000;        // "take the next stack entry"
 constexpr int kToTlas = (int)0x80000001;     // marker: leave the BLAS
 
@@ -345,7 +345,7 @@ __device__ __forceinline__ void rayInit(RayCtx& r, float3 o, float3 d, bool tri)
   if (tri) r.wt = wtSetup(d);
 }
 
-constexpr int kCwStack = 48;
+constexpr int kCwStack = kCwTraversalStack;
 constexpr uint32_t kGroupPrims = 1u << 31;   // entry holds a primitive group
 constexpr uint32_t kGroupMarker = 1u << 30;  // entry returns from a BLAS
 
@@ -407,8 +407,8 @@ __device__ SDB_TRAVERSE_INLINE bool traverse(const SdLaunch& lp, float3 O, float
         float3 o2 = xfPoint(in.w2o, O), d2 = xfVec(in.w2o, D);
         if (in.kind == GK_MESH) {
           if (COUNT) cnt->blasEntries++;
-          // No room to suspend this level (deeper than any tree the builder
-          // makes): skip the instance rather than overflow.
+          // Unreachable: the scene build rejects trees whose TLAS + BLAS
+          // depth could fill the stack (kCwTraversalStack).
           if (sp + 3 > kCwStack) continue;
           if (gHits) stack[sp++] = make_uint2(gBase, gHits | (gImask << 8));
           if (tBits) stack[sp++] = make_uint2(tBase, tBits | kGroupPrims);

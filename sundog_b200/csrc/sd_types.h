@@ -138,6 +138,15 @@ struct __align__(16) CwNode {
 };
 constexpr int kCwLeafMax = 3;  // primitives per leaf slot
 
+// Traversal stack entries (sd_trace.cuh, wavefront.cu). The binary walk
+// pushes at most one entry per inner level plus one marker at a BLAS entry,
+// so TLAS depth + BLAS depth + 2 <= kTraversalStack; the 8-wide walk pushes
+// at most one group per level plus three entries at a BLAS entry, so
+// TLAS depth + BLAS depth + 4 <= kCwTraversalStack. The scene build rejects
+// deeper trees, so no traversal ever finds its stack full.
+constexpr int kTraversalStack = 64;
+constexpr int kCwTraversalStack = 48;
+
 // Everything a launch needs, in constant memory.
 struct SdLaunch {
   int width, height;

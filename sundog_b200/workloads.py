@@ -312,6 +312,44 @@ CONFIGS = {
 }
 
 
+def features():
+    """Feature coverage at 72x48, 8 spp: every quadric kind, checker and grid
+    textures, Lambert / metal / glass / rough glass / plastic / water
+    materials, an emissive rect (auto NEE), a soft point light, a distant
+    light, a thin-lens camera and a gradient sky."""
+    s = Scene()
+    s.render(width=72, height=48, spp=8, max_depth=8, seed=3, clamp=0.0)
+    s.camera(lookfrom=[0, 3.0, 8.5], lookat=[0, 0.9, 0], vfov=40, aperture=0.03)
+    s.background_gradient(horizon=[0.9, 0.9, 0.95], zenith=[0.35, 0.55, 0.95])
+    s.texture("floor", "checker", a=[0.8, 0.8, 0.8], b=[0.25, 0.25, 0.3], scale=[12, 12])
+    s.texture("lines", "grid", a=[0.7, 0.6, 0.5], b=[0.1, 0.1, 0.1], scale=[6, 6], width=0.08)
+    s.lambert("ground", texture="floor")
+    s.lambert("red", color=[0.75, 0.25, 0.25])
+    s.lambert("gridded", texture="lines")
+    s.metal("gold", color=[1.0, 0.78, 0.34], roughness=0.15)
+    s.metal("mirror", color=[0.9, 0.9, 0.9], roughness=0.0)
+    s.dielectric("glass", ior=1.5)
+    s.dielectric("frost", ior=1.45, roughness=0.3, absorb=[0.1, 0.2, 0.3])
+    s.plastic("toy", color=[0.2, 0.5, 0.8], roughness=0.2)
+    s.water("pool", absorb=[0.3, 0.1, 0.05])
+    s.emissive("lamp", color=[1.0, 0.95, 0.85], intensity=20.0)
+    s.point_light(position=[5, 5, 4], intensity=[30, 30, 30], radius=0.3)
+    s.distant_light(direction=[-0.5, -1, -0.3], radiance=[0.6, 0.6, 0.55])
+    s.add("rect", "ground", scale(8))
+    s.add("sphere", "glass", scale(0.8), translate(-3.0, 0.8, 1.0))
+    s.add("sphere", "red", scale(0.8), translate(-1.0, 0.8, 1.0))
+    s.add("cylinder", "gold", scale(0.6, 0.8, 0.6), translate(1.0, 0.8, 1.0))
+    s.add("parabola", "mirror", scale(1.4, 1.4, 1.4), rotate_z(90), translate(3.4, 1.4, 0.0),
+          material_back=None)
+    s.add("disk", "mirror", scale(1.6), rotate_x(90), translate(0, 1.6, -3.2))
+    s.add("rect", "lamp", rotate_x(180), scale(1.2), translate(0, 6, 2))
+    s.add("sphere", "frost", scale(0.5, 0.7, 0.5), translate(2.2, 0.7, 2.4))
+    s.add("sphere", "toy", scale(0.45), rotate_y(30), translate(-2.0, 0.45, 2.6))
+    s.add("rect", "gridded", scale(1.0, 1, 0.6), rotate_x(70), translate(-3.5, 1.0, -2.0))
+    s.add("rect", "pool", scale(1.2), translate(0.2, 0.05, 3.2))
+    return s
+
+
 def make(config, asset_dir, **kw):
     if config == 0:
         return cornell(**kw)

@@ -7,8 +7,6 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
-
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); parity tests of the sm_100a path")
@@ -35,6 +33,3 @@ def oracle_lib():
 def asset_dir(tmp_path_factory):
     return str(tmp_path_factory.mktemp("assets"))
 
-
-def reference_present():
-    return os.path.isdir(os.path.join(REFERENCE, "scenes"))

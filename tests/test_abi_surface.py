@@ -103,7 +103,9 @@ def test_last_error_is_per_thread(lib):
     lib.sundog_scene_destroy(h)
 
 
-REF_SCENES = "/root/reference/scenes"
+from oracle.refpath import reference_root
+
+REF_SCENES = os.path.join(reference_root() or "", "scenes")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_SCENES), reason="reference sources not mounted")

@@ -1,8 +1,8 @@
 """The allocation-free tile render (sundog_session_render_tile_noalloc).
 
 It exists for callers that cannot allocate device memory while they render
-(a worker whose device memory belongs to another allocator, code recorded
-into a CUDA graph); its scratch is a static device array inside the library.
+(a worker whose device memory belongs to another allocator or is held to a
+fixed budget); its scratch is a static device array inside the library.
 Here the caller's film is a torch tensor (memory the caller already owns).
 Checked against the existing entry point (a full render of the same session
 read back with sundog_session_read) on consecutive calls that reuse the
@@ -74,3 +74,29 @@ def test_tile_noalloc_rejects_oversized_and_outside(lib):
         rc = lib.sundog_session_render_tile_noalloc(ses.handle, 40, 0, 32, 16, 0, 4,
                                                     film.data_ptr(), None, None)
         assert rc != 0 and b"outside" in lib.sundog_last_error()
+
+
+def test_tile_noalloc_follows_session_sample_offset(lib):
+    """A session created with a sample offset draws samples offset..offset+spp;
+    the tile call counts its sample_begin from that offset too."""
+    torch = pytest.importorskip("torch")
+    s = workloads.cornell(width=48, height=32, spp=8)
+    with sc.Session(s, sample_offset=5) as ses:
+        ses.render()
+        full = ses.read()
+        f, _ = tile(lib, ses, 0, 0, 48, 32, 0, 8)
+        assert close(f.cpu().numpy(), full) == 1.0
+    with sc.Session(s) as plain:
+        plain.render()
+        assert not np.array_equal(plain.read(), full)
+
+
+def test_tile_noalloc_rejects_guided_session(lib):
+    torch = pytest.importorskip("torch")
+    s = workloads.cornell(width=32, height=32, spp=4)
+    with sc.Session(s) as ses:
+        ses.set_guiding(True)
+        film = torch.zeros((32, 32, 4), dtype=torch.float32, device="cuda")
+        rc = lib.sundog_session_render_tile_noalloc(ses.handle, 0, 0, 32, 32, 0, 4,
+                                                    film.data_ptr(), None, None)
+        assert rc != 0 and b"guiding" in lib.sundog_last_error()
