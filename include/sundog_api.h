@@ -275,6 +275,28 @@ typedef struct {
   uint64_t loop_lanes;    /* lanes running a path segment in them */
 } sundog_trace_counts;
 SUNDOG_API int sundog_session_trace_counts(sundog_session*, sundog_trace_counts*);
+/* The same counting render with the two ray kinds apart: radiance rays
+ * (camera and bounce rays, closest hit) in *radiance and shadow rays (any hit,
+ * transparent crossings) in *shadow; `rays` of each is its traversal count and
+ * loop_* are only filled for the radiance set (the path loop). No counterpart
+ * in the reference. Returns 0/1. */
+SUNDOG_API int sundog_session_trace_counts_split(sundog_session*, sundog_trace_counts* radiance,
+                                                 sundog_trace_counts* shadow);
+
+/* Per-stage device time of a session's wavefront renders (no counterpart in
+ * the reference). With stage timing on, each later session_render records
+ * CUDA events around every stage launch on its stream (read at the
+ * synchronisation the engine makes once per iteration) and keeps, for the
+ * last render: the summed milliseconds of the start, trace (radiance rays),
+ * shade-A, shadow-ray and shade-B stages, the iterations, the radiance and
+ * shadow rays traced and the stage launches. Megakernel renders leave it
+ * zero. Returns 0/1. */
+typedef struct {
+  double start_ms, trace_ms, shade_a_ms, shadow_ms, shade_b_ms;
+  uint64_t iterations, radiance_rays, shadow_rays, launches;
+} sundog_stage_times;
+SUNDOG_API int sundog_session_set_stage_timing(sundog_session*, int enable);
+SUNDOG_API int sundog_session_stage_times(sundog_session*, sundog_stage_times*);
 
 /* Allocation-free tile render (no counterpart in the reference). For callers
  * that cannot allocate device memory when they render, such as a serving

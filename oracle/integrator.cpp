@@ -15,6 +15,7 @@
 // Scene input is a line-oriented text description (written by
 // oracle/oracle.py from the parse-time scene state); see sdo_scene_load.
 #include <algorithm>
+#include <cctype>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -77,6 +78,60 @@ struct Scene {
 };
 
 // ---- assets ---------------------------------------------------------------------
+
+// Binary PPM (P6, maxval 255) or PAM (P7, DEPTH 3 or 4, MAXVAL 255) as RGBA8,
+// row 0 = top; alpha 255 where the file has none. The oracle's own reader of
+// the uncompressed formats the tests write (the reference decodes AVIF with
+// libavif into the same RGBA8 layout, src/textures.cpp:22-64).
+std::vector<unsigned char> loadImageRgba8(const std::string& path, int& w, int& h) {
+  std::unique_ptr<FILE, int (*)(FILE*)> f(std::fopen(path.c_str(), "rb"), &std::fclose);
+  if (!f) throw std::runtime_error("oracle: cannot open " + path);
+  // Next whitespace-separated header token, skipping '#' comments.
+  auto token = [&]() {
+    std::string t;
+    int c;
+    while ((c = std::fgetc(f.get())) != EOF) {
+      if (c == '#' && t.empty()) {
+        while (c != EOF && c != '\n') c = std::fgetc(f.get());
+      } else if (std::isspace(c)) {
+        if (!t.empty()) return t;
+      } else {
+        t.push_back((char)c);
+      }
+    }
+    if (t.empty()) throw std::runtime_error("oracle: truncated header in " + path);
+    return t;
+  };
+  std::string magic = token();
+  int depth = 0;
+  w = h = 0;
+  if (magic == "P6") {
+    w = std::atoi(token().c_str());
+    h = std::atoi(token().c_str());
+    if (std::atoi(token().c_str()) != 255) throw std::runtime_error("oracle: PPM maxval must be 255");
+    depth = 3;
+  } else if (magic == "P7") {
+    for (std::string k = token(); k != "ENDHDR"; k = token()) {
+      std::string v = token();
+      if (k == "WIDTH") w = std::atoi(v.c_str());
+      else if (k == "HEIGHT") h = std::atoi(v.c_str());
+      else if (k == "DEPTH") depth = std::atoi(v.c_str());
+      else if (k == "MAXVAL" && v != "255") throw std::runtime_error("oracle: PAM maxval must be 255");
+    }
+  } else {
+    throw std::runtime_error("oracle: unsupported image " + path);
+  }
+  if (w <= 0 || h <= 0 || (depth != 3 && depth != 4))
+    throw std::runtime_error("oracle: unsupported image header in " + path);
+  // token() consumed the one whitespace byte that ends the header.
+  std::vector<unsigned char> raw((size_t)w * h * depth);
+  if (std::fread(raw.data(), 1, raw.size(), f.get()) != raw.size())
+    throw std::runtime_error("oracle: truncated pixels in " + path);
+  std::vector<unsigned char> rgba((size_t)w * h * 4);
+  for (size_t i = 0; i < (size_t)w * h; i++)
+    for (int c = 0; c < 4; c++) rgba[4 * i + c] = c < depth ? raw[depth * i + c] : 255;
+  return rgba;
+}
 
 // OBJ reader with the reference loader's conventions (src/mesh_obj.cpp:13-145).
 void loadObj(const std::string& path, bool smooth, const std::string& usemtl, Mesh& out) {
@@ -346,7 +401,11 @@ std::unique_ptr<Scene> parseScene(const std::string& text) {
       std::string file;
       ss >> t.kind >> t.a.x >> t.a.y >> t.a.z >> t.b.x >> t.b.y >> t.b.z >> t.scale.x >> t.scale.y >> t.width >>
           t.srgb >> file;
-      if (t.kind == TX_IMAGE) throw std::runtime_error("oracle: image textures need the image loader");
+      if (t.kind == TX_IMAGE) {
+        S->texImg.push_back(loadImageRgba8(file, t.imgW, t.imgH));
+      } else {
+        S->texImg.emplace_back();
+      }
       S->tex.push_back(t);
     } else if (k == "material") {
       MaterialDesc m{};
@@ -387,7 +446,8 @@ std::unique_ptr<Scene> parseScene(const std::string& text) {
   }
   if (S->W <= 0 || S->H <= 0) throw std::runtime_error("oracle: missing render line");
   S->cam = makeCamera(lf, la, up, vfov, aperture, focus, S->W, S->H);
-  for (auto& t : S->tex) t.img = nullptr;
+  for (size_t i = 0; i < S->tex.size(); i++)
+    S->tex[i].img = S->tex[i].kind == TX_IMAGE ? S->texImg[i].data() : nullptr;
   // meshes
   S->meshes.resize(meshFiles.size());
   for (size_t i = 0; i < meshFiles.size(); i++) {

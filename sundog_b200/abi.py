@@ -86,6 +86,14 @@ class TraceCounts(ctypes.Structure):
                 ("loop_lanes", ctypes.c_uint64)]
 
 
+class StageTimes(ctypes.Structure):
+    _fields_ = [("start_ms", ctypes.c_double), ("trace_ms", ctypes.c_double),
+                ("shade_a_ms", ctypes.c_double), ("shadow_ms", ctypes.c_double),
+                ("shade_b_ms", ctypes.c_double), ("iterations", ctypes.c_uint64),
+                ("radiance_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64)]
+
+
 class GuidingConfig(ctypes.Structure):
     _fields_ = [("train_spp", ctypes.c_int32), ("pass_spp", ctypes.c_int32),
                 ("steps_per_pass", ctypes.c_int32), ("batch", ctypes.c_int32),
@@ -156,7 +164,8 @@ ADDITIVE_SYMBOLS = [
     "sundog_session_guide_records", "sundog_server_defaults", "sundog_server_create",
     "sundog_server_submit", "sundog_server_status", "sundog_server_wait",
     "sundog_server_cancel", "sundog_server_stats", "sundog_server_destroy",
-    "sundog_session_copy_film",
+    "sundog_session_copy_film", "sundog_session_trace_counts_split",
+    "sundog_session_set_stage_timing", "sundog_session_stage_times",
 ]
 
 _lib = None
@@ -229,6 +238,10 @@ def load(path=None):
     lib.sundog_session_info.argtypes = [vp, ctypes.POINTER(SessionStats)]
     lib.sundog_session_copy_film.argtypes = [vp, vp, vp]
     lib.sundog_session_trace_counts.argtypes = [vp, ctypes.POINTER(TraceCounts)]
+    lib.sundog_session_trace_counts_split.argtypes = [vp, ctypes.POINTER(TraceCounts),
+                                                      ctypes.POINTER(TraceCounts)]
+    lib.sundog_session_set_stage_timing.argtypes = [vp, ip]
+    lib.sundog_session_stage_times.argtypes = [vp, ctypes.POINTER(StageTimes)]
     lib.sundog_transfer_bytes.argtypes = [ctypes.POINTER(ctypes.c_uint64)] * 2
     lib.sundog_transfer_bytes.restype = None
     lib.sundog_session_render_tile_noalloc.argtypes = [vp, ip, ip, ip, ip, ip, ip, vp,

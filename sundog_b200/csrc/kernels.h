@@ -27,7 +27,6 @@ int renderGridSize();
 // guide: 0 plain; kGuideSample / kGuideRecord bits select the guided variants.
 cudaError_t launchRender(cudaStream_t st, int grid, int guide = 0);
 cudaError_t launchFold(int npix, cudaStream_t st);
-struct TraceCount;  // sd_trace.cuh: four u64 counters
 // Same kernel with traversal visit counters (node box tests, triangle and
 // quadric tests, BLAS entries) summed into counts; for the roofline only.
 cudaError_t launchRenderCounting(cudaStream_t st, int grid, TraceCount* counts);

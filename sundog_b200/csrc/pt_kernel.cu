@@ -26,7 +26,9 @@ __constant__ SdLaunch c_lp;
 template <bool COUNT, int GUIDE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_MIN_BLOCKS) ptPersistent(TraceCount* counts) {
   const SdLaunch& lp = c_lp;
-  TraceCount cnt = {0, 0, 0, 0, 0, 0, 0, 0};
+  // Counting build: [0] radiance traversals and the path loop, [1] shadow
+  // traversals.
+  TraceCount cnt[2] = {{0, 0, 0, 0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0, 0, 0, 0}};
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned ltMask = (1u << lane) - 1u;
@@ -61,8 +63,8 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_MIN_BLOCKS) ptPersistent(Tra
       continue;
     }
     if (active) {
-      if (COUNT) countWarp(&cnt, cnt.loopIters, cnt.loopLanes);
-      if (!bounce<COUNT, GUIDE>(lp, p, rays, &cnt, &trail)) {
+      if (COUNT) countWarp(&cnt[0], cnt[0].loopIters, cnt[0].loopLanes);
+      if (!bounce<COUNT, GUIDE>(lp, p, rays, cnt, &trail)) {
         float3 L = sanitize3(p.L);
         if (GUIDE & kGuideRecord) guideFlush(lp, trail, L);
         lp.sampleL[p.slot] = make_float4(L.x, L.y, L.z, 1.0f);
@@ -74,14 +76,17 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_MIN_BLOCKS) ptPersistent(Tra
   for (int off = 16; off > 0; off >>= 1) rays += __shfl_down_sync(full, rays, off);
   if (lane == 0 && rays) atomicAdd(lp.rayCounter, rays);
   if (COUNT) {
-    atomicAdd(&counts->boxTests, cnt.boxTests);
-    atomicAdd(&counts->triTests, cnt.triTests);
-    atomicAdd(&counts->quadTests, cnt.quadTests);
-    atomicAdd(&counts->blasEntries, cnt.blasEntries);
-    atomicAdd(&counts->travIters, cnt.travIters);
-    atomicAdd(&counts->travLanes, cnt.travLanes);
-    atomicAdd(&counts->loopIters, cnt.loopIters);
-    atomicAdd(&counts->loopLanes, cnt.loopLanes);
+    for (int k = 0; k < 2; k++) {
+      atomicAdd(&counts[k].boxTests, cnt[k].boxTests);
+      atomicAdd(&counts[k].triTests, cnt[k].triTests);
+      atomicAdd(&counts[k].quadTests, cnt[k].quadTests);
+      atomicAdd(&counts[k].blasEntries, cnt[k].blasEntries);
+      atomicAdd(&counts[k].travIters, cnt[k].travIters);
+      atomicAdd(&counts[k].travLanes, cnt[k].travLanes);
+      atomicAdd(&counts[k].loopIters, cnt[k].loopIters);
+      atomicAdd(&counts[k].loopLanes, cnt[k].loopLanes);
+      atomicAdd(&counts[k].traces, cnt[k].traces);
+    }
   }
 }
 

@@ -421,7 +421,8 @@ __device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned lon
       rays++;
       float3 so = nudge(x, transmitNee ? -ns : ns);
       float tmaxS = ls.dist * 0.999f;
-      float3 tr = shadowTransmittance<COUNT>(lp, so, ls.wi, tmaxS, cnt);
+      // Counting build: shadow traversals go to the second counter set.
+      float3 tr = shadowTransmittance<COUNT>(lp, so, ls.wi, tmaxS, COUNT ? cnt + 1 : nullptr);
       if (hmax(tr) > 0.0f) {
         if (lp.numFlames > 0 && lp.transparentShadows) {
           int skip = k < lp.numLights ? lp.lights[k].flameId : -1;

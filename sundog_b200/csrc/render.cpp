@@ -630,6 +630,7 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
   }
   cudaCheck(cudaMemsetAsync(lp.rayCounter, 0, sizeof(unsigned long long), st), "counter reset");
   cudaCheck(cudaStreamSynchronize(st), "sync");
+  stages = WfStageTimes();
   auto t0 = Clock::now();
   cudaCheck(cudaEventRecord(ev0, st), "event");
   uint64_t launches = 0;
@@ -654,7 +655,7 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
     } else if (wavefront) {
       if (!wf) wf = wfAcquire();
       wf->ensure((int)std::min<unsigned long long>(lp.numPaths, kWavefrontSlots));
-      launches += wfRender(lp, *wf, st, mode);
+      launches += wfRender(lp, *wf, st, mode, stageTiming ? &stages : nullptr);
     } else {
       cudaCheck(launchRender(st, grid, mode), "path kernel launch");
       launches += 1;
@@ -695,9 +696,9 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
   }
 }
 
-void RenderSession::countTraversal(sundog_trace_counts* out) {
+void RenderSession::countTraversal(sundog_trace_counts* out, sundog_trace_counts* shadow) {
   DevBuf dc;
-  dc.alloc(sizeof(unsigned long long) * 8);
+  dc.alloc(2 * sizeof(TraceCount));
   cudaCheck(cudaMemset(dc.ptr, 0, dc.bytes), "counter reset");
   cudaCheck(cudaMemsetAsync(accum.ptr, 0, accum.bytes, stream), "film reset");
   cudaCheck(cudaMemsetAsync(lp.rayCounter, 0, sizeof(unsigned long long), stream), "counter reset");
@@ -715,18 +716,29 @@ void RenderSession::countTraversal(sundog_trace_counts* out) {
     done += n;
   }
   cudaCheck(cudaStreamSynchronize(stream), "counting render");
-  unsigned long long c[8], rays = 0;
+  TraceCount c[2];
+  unsigned long long rays = 0;
   cudaCheck(cudaMemcpy(c, dc.ptr, sizeof c, cudaMemcpyDeviceToHost), "counts");
   cudaCheck(cudaMemcpy(&rays, lp.rayCounter, sizeof rays, cudaMemcpyDeviceToHost), "ray count");
-  out->rays = rays;
-  out->box_tests = c[0];
-  out->tri_tests = c[1];
-  out->quadric_tests = c[2];
-  out->blas_entries = c[3];
-  out->trav_iters = c[4];
-  out->trav_lanes = c[5];
-  out->loop_iters = c[6];
-  out->loop_lanes = c[7];
+  auto put = [](sundog_trace_counts* o, const TraceCount& a, const TraceCount* b,
+                unsigned long long r) {
+    o->rays = r;
+    o->box_tests = a.boxTests + (b ? b->boxTests : 0);
+    o->tri_tests = a.triTests + (b ? b->triTests : 0);
+    o->quadric_tests = a.quadTests + (b ? b->quadTests : 0);
+    o->blas_entries = a.blasEntries + (b ? b->blasEntries : 0);
+    o->trav_iters = a.travIters + (b ? b->travIters : 0);
+    o->trav_lanes = a.travLanes + (b ? b->travLanes : 0);
+    o->loop_iters = a.loopIters;
+    o->loop_lanes = a.loopLanes;
+  };
+  if (!shadow) {
+    put(out, c[0], &c[1], rays);  // both ray kinds together
+  } else {
+    put(out, c[0], nullptr, c[0].traces);
+    put(shadow, c[1], nullptr, c[1].traces);
+    shadow->loop_iters = shadow->loop_lanes = 0;
+  }
 }
 
 void RenderSession::read(float* film, float* alb, float* nrm) {
@@ -851,6 +863,40 @@ extern "C" int sundog_session_trace_counts(sundog_session* sh, sundog_trace_coun
   SDB_TRY
   if (!sh || !out) throw std::runtime_error("session: null argument");
   reinterpret_cast<RenderSession*>(sh)->countTraversal(out);
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_session_set_stage_timing(sundog_session* sh, int enable) {
+  SDB_TRY
+  if (!sh) throw std::runtime_error("stage timing: null session");
+  reinterpret_cast<RenderSession*>(sh)->stageTiming = enable != 0;
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_session_stage_times(sundog_session* sh, sundog_stage_times* out) {
+  SDB_TRY
+  if (!sh || !out) throw std::runtime_error("stage times: null argument");
+  const WfStageTimes& t = reinterpret_cast<RenderSession*>(sh)->stages;
+  out->start_ms = t.startMs;
+  out->trace_ms = t.traceMs;
+  out->shade_a_ms = t.shadeAMs;
+  out->shadow_ms = t.shadowMs;
+  out->shade_b_ms = t.shadeBMs;
+  out->iterations = t.iterations;
+  out->radiance_rays = t.radianceRays;
+  out->shadow_rays = t.shadowRays;
+  out->launches = t.launches;
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_session_trace_counts_split(sundog_session* sh, sundog_trace_counts* radiance,
+                                                 sundog_trace_counts* shadow) {
+  SDB_TRY
+  if (!sh || !radiance || !shadow) throw std::runtime_error("trace counts: null argument");
+  reinterpret_cast<RenderSession*>(sh)->countTraversal(radiance, shadow);
   return SUNDOG_OK;
   SDB_CATCH(SUNDOG_ERROR)
 }

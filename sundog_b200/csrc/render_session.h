@@ -14,6 +14,15 @@ namespace sdb {
 
 void cudaCheck(cudaError_t e, const char* what);
 
+// Per-stage device time of wavefront renders, accumulated while a session
+// has stage timing on: CUDA events on the render stream around each stage
+// launch, read at the per-iteration synchronisation the engine makes anyway.
+struct WfStageTimes {
+  double startMs = 0, traceMs = 0, shadeAMs = 0, shadowMs = 0, shadeBMs = 0;
+  unsigned long long iterations = 0, radianceRays = 0, shadowRays = 0, launches = 0;
+};
+
+
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
@@ -104,12 +113,16 @@ struct RenderSession {
   std::unique_ptr<GuideState> guide;  // learned path guiding, when enabled
   std::unique_ptr<WfBuffers> wf;      // wavefront slot pool, when used
   int engine = 0;                     // sundog_render_ext.engine
+  bool stageTiming = false;           // sundog_session_set_stage_timing
+  WfStageTimes stages;                // per-stage times of the last render
 
   ~RenderSession();
   void build(const sundog_scene* h, const sundog_render_options* opt, const sundog_render_ext* ext);
   void render(cudaStream_t st, bool reset, sundog_render_result* res);
   void read(float* film, float* alb, float* nrm);
-  void countTraversal(sundog_trace_counts* out);
+  // Counting render: traversal visit counts of both ray kinds in *out, or,
+  // with `shadow`, radiance rays in *out and shadow rays in *shadow.
+  void countTraversal(sundog_trace_counts* out, sundog_trace_counts* shadow = nullptr);
   void setGuiding(bool enable, const sundog_guiding_config* cfg);
 };
 

@@ -41,14 +41,6 @@ struct TraceHit {
   bool front;
 };
 
-// Visit counts of the traversal, gathered only by the counting variant of the
-// path kernel (for the algorithmic-bytes roofline), never in timed launches.
-struct TraceCount {
-  unsigned long long boxTests, triTests, quadTests, blasEntries;
-  // SIMT occupancy of the loops, summed by the first active lane of each
-  // warp: iterations executed, and active lanes over those iterations.
-  unsigned long long travIters, travLanes, loopIters, loopLanes;
-};
 
 __device__ __forceinline__ void countWarp(TraceCount* cnt, unsigned long long& iters,
                                           unsigned long long& lanes) {
@@ -368,6 +360,7 @@ template <bool SHADOW, bool COUNT = false>
 __device__ SDB_TRAVERSE_INLINE bool traverse(const SdLaunch& lp, float3 O, float3 D, float tmax,
                                              TraceHit& hit, float& trProd, float3& tau,
                                              TraceCount* cnt = nullptr) {
+  if (COUNT) cnt->traces++;
   if (lp.numInstances == 0) return SHADOW;
   uint2 stack[kCwStack];
   int sp = 0;
@@ -520,6 +513,7 @@ template <bool SHADOW, bool COUNT = false>
 __device__ SDB_TRAVERSE_INLINE bool traverse(const SdLaunch& lp, float3 O, float3 D, float tmax,
                                          TraceHit& hit, float& trProd, float3& tau,
                                          TraceCount* cnt = nullptr) {
+  if (COUNT) cnt->traces++;
   if (lp.numInstances == 0) return SHADOW;
   int stack[kStackSize];
   int sp = 0;

@@ -147,6 +147,16 @@ constexpr int kCwLeafMax = 3;  // primitives per leaf slot
 constexpr int kTraversalStack = 64;
 constexpr int kCwTraversalStack = 48;
 
+// Visit counts of the traversal, gathered only by the counting variant of the
+// path kernel (for the algorithmic-bytes roofline), never in timed launches.
+struct TraceCount {
+  unsigned long long boxTests, triTests, quadTests, blasEntries;
+  // SIMT occupancy of the loops, summed by the first active lane of each
+  // warp: iterations executed, and active lanes over those iterations.
+  unsigned long long travIters, travLanes, loopIters, loopLanes;
+  unsigned long long traces;  // traversals (rays) counted here
+};
+
 // Everything a launch needs, in constant memory.
 struct SdLaunch {
   int width, height;

@@ -168,6 +168,172 @@ __global__ void __launch_bounds__(kRenderBlock) wfStart() {
 // (sd_trace.cuh) in the same order with the same tests: the same closest
 // accepted hit. (Shadow rays, shorter, gained nothing from it.) SERVE: a
 // serving batch, each lane tracing in its own job's scene.
+#if SDB_WIDE_BVH
+// The same stage over the compressed 8-wide BVH (CwNode, sd_trace.cuh): each
+// loop iteration a lane either tests one primitive of its current leaf group
+// (a triangle, or a TLAS instance: quadric roots or entry into its BLAS),
+// tests the 8 child boxes of the nearest remaining child node, or pops a
+// group. The visit order and tests are those of traverse<false> in the
+// 8-wide build: the same closest accepted hit.
+template <bool SERVE>
+__global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetch(int in) {
+  const WfPool& pool = c_pool;
+  const unsigned n = pool.counts[in];
+  const unsigned full = 0xFFFFFFFFu;
+  const unsigned ltMask = (1u << (threadIdx.x & 31)) - 1u;
+  int job = 0;  // SERVE: the lane's job slot
+  const float tmin = 0.0f;
+  unsigned long long rays = 0;
+  int slot = -1;
+  bool exhausted = false;  // warp-uniform
+  float3 O = v3(0.0f), D = v3(0.0f);
+  RayCtx ray;
+  rayInit(ray, O, v3(1.0f), false);
+  float tmax = 0.0f;
+  TraceHit hit;
+  bool found = false, inBlas = false;
+  int curInst = -1, sp = 0;
+  uint32_t gBase = 0, gHits = 0, gImask = 0, tBase = 0, tBits = 0;
+  uint2 stack[kCwStack];
+  while (true) {
+    const unsigned idle = __ballot_sync(full, slot < 0);
+    if (!exhausted && (idle == full || __popc(idle) >= SDB_WF_FETCH_IDLE)) {
+      const int leader = __ffs(idle) - 1;
+      unsigned base = 0;
+      if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&pool.counts[3], (unsigned)__popc(idle));
+      base = __shfl_sync(full, base, leader);
+      if (base + __popc(idle) >= n) exhausted = true;
+      if (slot < 0) {
+        unsigned i = base + __popc(idle & ltMask);
+        if (i < n) {
+          slot = pool.lists[in][i];
+          if (SERVE) job = pool.jobs[slot];
+          const SdLaunch& jl = SERVE ? c_wjobs[job] : c_wlp;
+          O = pool.paths[slot].v.o;
+          D = pool.paths[slot].v.d;
+          rayInit(ray, O, D, false);
+          tmax = 1e16f;
+          found = false;
+          inBlas = false;
+          curInst = -1;
+          sp = 0;
+          gBase = (uint32_t)jl.tlasRoot;
+          gHits = jl.numInstances > 0 ? 1u << (0u ^ ray.rayOct) : 0u;
+          gImask = 1u;
+          tBits = 0;
+        }
+      }
+    }
+    if (__ballot_sync(full, slot >= 0) == 0) {
+      if (exhausted) break;
+      continue;
+    }
+    if (slot < 0) continue;
+    const SdLaunch& lp = SERVE ? c_wjobs[job] : c_wlp;
+    if (tBits) {
+      const int j = __ffs(tBits) - 1;
+      tBits &= tBits - 1u;
+      const int prim = (int)tBase + j;
+      if (!inBlas) {
+        const SdInstance& inst = lp.inst[prim];
+        float3 o2 = xfPoint(inst.w2o, O), d2 = xfVec(inst.w2o, D);
+        if (inst.kind == GK_MESH) {
+          // Suspend this level (the scene build keeps TLAS + BLAS depth
+          // within the stack) and walk the BLAS in object space.
+          if (sp + 3 > kCwStack) continue;
+          if (gHits) stack[sp++] = make_uint2(gBase, gHits | (gImask << 8));
+          if (tBits) stack[sp++] = make_uint2(tBase, tBits | kGroupPrims);
+          stack[sp++] = make_uint2(0xFFFFFFFFu, kGroupMarker);
+          inBlas = true;
+          curInst = prim;
+          rayInit(ray, o2, d2, true);
+          gBase = (uint32_t)lp.meshes[inst.mesh].root;
+          gHits = 1u << (0u ^ ray.rayOct);
+          gImask = 1u;
+          tBits = 0;
+          continue;
+        }
+        QHits qh = hitQuadric(inst.kind, o2, d2, tmin, tmax);
+        for (int k = 0; k < qh.n; k++) {
+          const QHit& q = qh.h[k];
+          if (q.t >= tmax) continue;
+          bool front = dot(q.n, d2) < 0.0f;
+          if ((inst.flags & kInstMasked) && !faceAccepts(lp, inst, front, q.u, q.v)) continue;
+          tmax = q.t;
+          found = true;
+          hit.t = q.t;
+          hit.inst = prim;
+          hit.prim = 0;
+          hit.u = q.u;
+          hit.v = q.v;
+          hit.nq = q.n;
+          hit.front = front;
+        }
+        continue;
+      }
+      // Triangle of the current BLAS, in object space.
+      const float4* tp = lp.tris + 3 * (size_t)prim;
+      float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+      float t, b1, b2;
+      float3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
+      if (!wtHit(ray.wt, ray.o, p0, p1, p2, tmin, tmax, t, b1, b2)) continue;
+      const int tri = __float_as_int(a.w);
+      const SdInstance& inst = lp.inst[curInst];
+      bool front;
+      if (!(inst.flags & (kInstMasked | kInstTransmissive))) {
+        front = dot(cross(p1 - p0, p2 - p0), ray.d) < 0.0f;
+      } else {
+        ShadePt spt = triShade(lp, inst, tri, b1, b2, D);
+        if ((inst.flags & kInstMasked) && !faceAccepts(lp, inst, spt.front, spt.u, spt.v)) continue;
+        front = spt.front;
+      }
+      tmax = t;
+      found = true;
+      hit.t = t;
+      hit.inst = curInst;
+      hit.prim = tri;
+      hit.u = b1;
+      hit.v = b2;
+      hit.front = front;
+      continue;
+    }
+    if (gHits) {
+      const int b = __ffs(gHits) - 1;
+      gHits &= gHits - 1u;
+      const uint32_t cs = (uint32_t)b ^ ray.rayOct;
+      const int child = (int)(gBase + __popc(gImask & ((1u << cs) - 1u)));
+      if (gHits && sp < kCwStack) stack[sp++] = make_uint2(gBase, gHits | (gImask << 8));
+      CwHits h = cwIntersect(lp.cw, child, ray.o, ray.id, ray.rayOct, tmin, tmax);
+      gBase = h.childBase;
+      gHits = h.hits;
+      gImask = h.imask;
+      tBase = h.primBase;
+      tBits = h.leafBits;
+      continue;
+    }
+    if (sp == 0) {  // ray done
+      if (!found) hit.inst = -1;
+      pool.hits[slot].v = hit;
+      rays++;
+      slot = -1;
+      continue;
+    }
+    const uint2 e = stack[--sp];
+    if (e.y & kGroupMarker) {
+      inBlas = false;
+      rayInit(ray, O, D, false);
+    } else if (e.y & kGroupPrims) {
+      tBase = e.x;
+      tBits = e.y & 0xFFFFFFu;
+    } else {
+      gBase = e.x;
+      gHits = e.y & 0xFFu;
+      gImask = (e.y >> 8) & 0xFFu;
+    }
+  }
+  addRays<SERVE ? kWfServe : 0>(rays);
+}
+#else
 template <bool SERVE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetch(int in) {
   const WfPool& pool = c_pool;
@@ -334,6 +500,7 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
   }
   addRays<SERVE ? kWfServe : 0>(rays);
 }
+#endif
 
 template <int GUIDE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeA(int in, int out) {
@@ -434,7 +601,7 @@ void WfBuffers::ensure(int slots) {
   shadow.alloc((size_t)slots * sizeof(int));
   jobs.alloc((size_t)slots);
   if (!counts.ptr) counts.alloc(4 * sizeof(unsigned));
-  if (!hostCount) cudaCheck(cudaMallocHost((void**)&hostCount, sizeof(unsigned)), "pinned count");
+  if (!hostCount) cudaCheck(cudaMallocHost((void**)&hostCount, 4 * sizeof(unsigned)), "pinned count");
   cap = slots;
   gridTrace = gridFor(wfTraceFetch<false>);
   gridShadeA = gridFor(wfShadeA<0>);
@@ -451,6 +618,8 @@ void WfBuffers::ensureTrails() {
 
 WfBuffers::~WfBuffers() {
   if (hostCount) cudaFreeHost(hostCount);
+  for (cudaEvent_t& e : ev)
+    if (e) cudaEventDestroy(e);
 }
 
 // One idle pool per device, kept between sessions: a one-shot render
@@ -483,18 +652,34 @@ size_t wfSlotBytes() {
 // Renders the launch block's paths (lp.numPaths ids, counters already
 // cleared) into lp.sampleL through the stages. Returns the kernels launched.
 // One iteration's stage kernels for mode GUIDE (guide bits, or kWfServe).
+// With `timed`, events ev[1..5] bracket the four stage launches.
 template <int GUIDE>
-static void wfIteration(const WfBuffers& b, cudaStream_t st, int cur, int nxt) {
+static void wfIteration(const WfBuffers& b, cudaStream_t st, int cur, int nxt, bool timed) {
+  if (timed) cudaEventRecord(b.ev[1], st);
   wfTraceFetch<(GUIDE & kWfServe) != 0><<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
+  if (timed) cudaEventRecord(b.ev[2], st);
   wfShadeA<GUIDE><<<b.gridShadeA, kRenderBlock, 0, st>>>(cur, nxt);
+  if (timed) cudaEventRecord(b.ev[3], st);
   wfShadow<GUIDE><<<b.gridShadow, kRenderBlock, 0, st>>>();
+  if (timed) cudaEventRecord(b.ev[4], st);
   wfShadeB<GUIDE><<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
+  if (timed) cudaEventRecord(b.ev[5], st);
+}
+
+static double evMs(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.0f;
+  cudaCheck(cudaEventElapsedTime(&ms, a, b), "stage timing");
+  return ms;
 }
 
 // Fills the pool with the first paths of ids [0, numPaths) and runs stage
 // iterations until no path is live (the launch block or batch is already in
 // constant memory). Returns the kernels launched.
-static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, int mode) {
+static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, int mode,
+                   WfStageTimes* times = nullptr) {
+  const bool timed = times != nullptr;
+  if (timed && !b.ev[0])
+    for (cudaEvent_t& e : b.ev) cudaCheck(cudaEventCreate(&e), "stage timing events");
   WfPool pool;
   pool.paths = (PoolSlot<Path>*)b.paths.ptr;
   pool.verts = (PoolSlot<Vertex>*)b.verts.ptr;
@@ -512,6 +697,7 @@ static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, i
             "wavefront pool");
   cudaCheck(cudaMemsetAsync(b.counts.ptr, 0, b.counts.bytes, st), "wavefront counts");
   int launches = 0;
+  if (timed) cudaEventRecord(b.ev[0], st);
   if (mode & kWfServe)
     wfStart<kWfServe><<<b.gridStart, kRenderBlock, 0, st>>>();
   else if (mode & kGuideRecord)
@@ -520,6 +706,12 @@ static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, i
     wfStart<0><<<b.gridStart, kRenderBlock, 0, st>>>();
   cudaCheck(cudaGetLastError(), "wfStart");
   launches++;
+  if (timed) {
+    cudaEventRecord(b.ev[1], st);
+    cudaCheck(cudaEventSynchronize(b.ev[1]), "wfStart");
+    times->startMs += evMs(b.ev[0], b.ev[1]);
+    times->launches++;
+  }
   unsigned* counts = (unsigned*)b.counts.ptr;
   int cur = 0;
   for (int iter = 0;; iter++) {
@@ -527,32 +719,43 @@ static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, i
     cudaCheck(cudaMemsetAsync(counts + nxt, 0, sizeof(unsigned), st), "wavefront counts");
     cudaCheck(cudaMemsetAsync(counts + 2, 0, 2 * sizeof(unsigned), st), "wavefront counts");
     switch (mode) {
-      case 0: wfIteration<0>(b, st, cur, nxt); break;
-      case kGuideSample: wfIteration<kGuideSample>(b, st, cur, nxt); break;
-      case kGuideRecord: wfIteration<kGuideRecord>(b, st, cur, nxt); break;
-      case kGuideSample | kGuideRecord: wfIteration<kGuideSample | kGuideRecord>(b, st, cur, nxt); break;
-      default: wfIteration<kWfServe>(b, st, cur, nxt); break;
+      case 0: wfIteration<0>(b, st, cur, nxt, timed); break;
+      case kGuideSample: wfIteration<kGuideSample>(b, st, cur, nxt, timed); break;
+      case kGuideRecord: wfIteration<kGuideRecord>(b, st, cur, nxt, timed); break;
+      case kGuideSample | kGuideRecord: wfIteration<kGuideSample | kGuideRecord>(b, st, cur, nxt, timed); break;
+      default: wfIteration<kWfServe>(b, st, cur, nxt, timed); break;
     }
     cudaCheck(cudaGetLastError(), "wavefront stage");
     launches += 4;
     cur = nxt;
-    cudaCheck(cudaMemcpyAsync(b.hostCount, counts + cur, sizeof(unsigned), cudaMemcpyDeviceToHost,
-                              st),
+    // All four counters: [cur] is now the next iteration's live list, [1 - cur]
+    // the list this iteration traced, [2] its shadow rays.
+    cudaCheck(cudaMemcpyAsync(b.hostCount, counts, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, st),
               "wavefront count");
     cudaCheck(cudaStreamSynchronize(st), "wavefront iteration");
-    if (*b.hostCount == 0) break;
+    if (timed) {
+      times->traceMs += evMs(b.ev[1], b.ev[2]);
+      times->shadeAMs += evMs(b.ev[2], b.ev[3]);
+      times->shadowMs += evMs(b.ev[3], b.ev[4]);
+      times->shadeBMs += evMs(b.ev[4], b.ev[5]);
+      times->iterations++;
+      times->launches += 4;
+      times->radianceRays += b.hostCount[1 - cur];
+      times->shadowRays += b.hostCount[2];
+    }
+    if (b.hostCount[cur] == 0) break;
     if (iter > (1 << 24)) throw std::runtime_error("wavefront: no progress");
   }
   return launches;
 }
 
-int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide) {
+int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide, WfStageTimes* times) {
   if (guide < 0 || guide > (kGuideSample | kGuideRecord))
     throw std::runtime_error("wavefront: invalid guide mode");
   if (guide & kGuideRecord) b.ensureTrails();
   cudaCheck(cudaMemcpyToSymbolAsync(c_wlp, &lp, sizeof lp, 0, cudaMemcpyHostToDevice, st),
             "wavefront launch block");
-  return runPool(b, st, lp.numPaths, guide);
+  return runPool(b, st, lp.numPaths, guide, times);
 }
 
 cudaError_t wfSetJob(int slot, const SdLaunch& lp, cudaStream_t st) {

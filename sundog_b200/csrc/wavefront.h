@@ -45,7 +45,8 @@ struct WfPool {
 struct WfBuffers {
   DevBuf paths, verts, hits, trs, pending, list0, list1, shadow, counts, jobs;
   DevBuf trails;  // allocated by the first training-record pass
-  unsigned* hostCount = nullptr;
+  unsigned* hostCount = nullptr;   // pinned: the four list counters
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // stage timing
   int cap = 0;
   int trailCap = 0;
   int gridStart = 0, gridTrace = 0, gridShadeA = 0, gridShadow = 0, gridShadeB = 0;
@@ -69,7 +70,9 @@ void wfRelease(std::unique_ptr<WfBuffers> b);
 // kGuideSample (draw directions by MIS with the learned guide of lp) and
 // kGuideRecord (keep each path's guided vertices in its slot's trail and turn
 // them into training records when the path ends).
-int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide = 0);
+// times: when non-null, per-stage event times and ray counts are added to it.
+int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide = 0,
+             WfStageTimes* times = nullptr);
 
 // Serving batches (serve.h): job slot `slot` of the engine's job table, and
 // one batch of tile-passes rendered through the pool into batch.sampleL at

@@ -304,6 +304,102 @@ def volumes(asset_dir, width=2560, height=1440, spp=256, flame_steps=64):
     return s
 
 
+def write_ppm(path, rgb8):
+    """Binary PPM (P6), row 0 = top."""
+    h, w, _ = rgb8.shape
+    with open(path, "wb") as f:
+        f.write(("P6\n%d %d\n255\n" % (w, h)).encode())
+        f.write(np.ascontiguousarray(rgb8, np.uint8).tobytes())
+
+
+def write_pam(path, rgba8):
+    """Binary PAM (P7) with an alpha channel, row 0 = top."""
+    h, w, _ = rgba8.shape
+    with open(path, "wb") as f:
+        f.write(("P7\nWIDTH %d\nHEIGHT %d\nDEPTH 4\nMAXVAL 255\nTUPLTYPE RGB_ALPHA\nENDHDR\n"
+                 % (w, h)).encode())
+        f.write(np.ascontiguousarray(rgba8, np.uint8).tobytes())
+
+
+def write_textured_assets(asset_dir):
+    """Images and a uv-mapped mesh for the textured scene: a 96x64 sRGB
+    colour ramp with a seeded speckle, a 40x40 linear (non-sRGB) stripe
+    image, a 64x64 RGBA leaf mask (alpha 0 outside a lobed outline and in
+    round holes) and a 4x4-quad uv grid mesh."""
+    os.makedirs(asset_dir, exist_ok=True)
+    ramp = os.path.join(asset_dir, "tex_ramp.ppm")
+    if not os.path.exists(ramp):
+        rng = np.random.default_rng(11)
+        y, x = np.mgrid[0:64, 0:96]
+        img = np.stack([x * 255 / 95, y * 255 / 63, 128 + 100 * np.sin(x * 0.3) * np.cos(y * 0.2)], -1)
+        img = np.clip(img + rng.integers(-20, 21, img.shape), 0, 255)
+        write_ppm(ramp, img.astype(np.uint8))
+    stripes = os.path.join(asset_dir, "tex_stripes.ppm")
+    if not os.path.exists(stripes):
+        y, x = np.mgrid[0:40, 0:40]
+        band = ((x + y) // 5) % 2
+        img = np.stack([200 * band + 30, 60 + 0 * x, 220 - 180 * band], -1)
+        write_ppm(stripes, img.astype(np.uint8))
+    leaf = os.path.join(asset_dir, "tex_leaf.pam")
+    if not os.path.exists(leaf):
+        y, x = np.mgrid[0:64, 0:64]
+        u, v = (x - 31.5) / 32.0, (y - 31.5) / 32.0
+        r, a = np.hypot(u, v), np.arctan2(v, u)
+        inside = r < 0.75 + 0.2 * np.cos(5 * a)
+        holes = np.hypot(u - 0.25, v + 0.1) < 0.12
+        holes |= np.hypot(u + 0.3, v - 0.3) < 0.1
+        alpha = np.where(inside & ~holes, 255, 0)
+        img = np.stack([40 + 60 * (u + 1), 150 + 40 * v, 50 + 0 * u, alpha], -1)
+        write_pam(leaf, np.clip(img, 0, 255).astype(np.uint8))
+    grid = os.path.join(asset_dir, "uv_grid.obj")
+    if not os.path.exists(grid):
+        n = 4
+        with open(grid, "w") as f:
+            f.write("# generated by sundog_b200.workloads: %dx%d quads with uv\n" % (n, n))
+            for j in range(n + 1):
+                for i in range(n + 1):
+                    f.write("v %.6f %.6f 0\n" % (i / n - 0.5, j / n - 0.5))
+                    f.write("vt %.6f %.6f\n" % (i / n, j / n))
+            for j in range(n):
+                for i in range(n):
+                    a = j * (n + 1) + i + 1
+                    b, c, d = a + 1, a + n + 1, a + n + 2
+                    f.write("f %d/%d %d/%d %d/%d\n" % (a, a, b, b, d, d))
+                    f.write("f %d/%d %d/%d %d/%d\n" % (a, a, d, d, c, c))
+    return ramp, stripes, leaf, grid
+
+
+def textured(asset_dir, width=96, height=64, spp=16):
+    """Image textures and alpha cutouts: an sRGB image on the floor, a linear
+    image on a sphere, an image-textured emissive rect (textured NEE light),
+    a cutout leaf on a rect and on a uv-mapped triangle mesh in front of a
+    point light (cutout shadows), and a glass sphere."""
+    ramp, stripes, leaf, grid = write_textured_assets(asset_dir)
+    s = Scene()
+    s.render(width=width, height=height, spp=spp, max_depth=8, seed=5, clamp=0.0)
+    s.camera(lookfrom=[0, 2.2, 6.5], lookat=[0, 0.8, 0], vfov=42)
+    s.background_gradient(horizon=[0.6, 0.65, 0.7], zenith=[0.2, 0.3, 0.5])
+    s.texture("ramp", "image", file=os.path.basename(ramp))
+    s.texture("stripes", "image", file=os.path.basename(stripes), srgb=False)
+    s.texture("leafmask", "image", file=os.path.basename(leaf))
+    s.lambert("floor", texture="ramp")
+    s.lambert("striped", texture="stripes")
+    s.lambert("leaf", texture="leafmask")
+    s.plastic("leafgloss", texture="leafmask", roughness=0.3)
+    s.emissive("sign", texture="ramp", intensity=4.0)
+    s.dielectric("glass", ior=1.5)
+    s.mesh("grid", os.path.basename(grid), normals="flat")
+    s.point_light(position=[1.5, 4.0, 2.5], intensity=[40, 38, 34], radius=0.2)
+    s.add("rect", "floor", scale(5))
+    s.add("sphere", "striped", scale(0.7), rotate_y(25), translate(-1.6, 0.7, 0.2))
+    s.add("sphere", "glass", scale(0.5), translate(1.7, 0.5, 0.9))
+    s.add("rect", "sign", scale(1.0, 1, 0.5), rotate_x(90), translate(1.6, 1.4, -2.0))
+    s.add("rect", "leaf", scale(0.9), rotate_x(70), translate(0.4, 1.5, 1.2),
+          cutout="leafmask")
+    s.add("mesh:grid", "leafgloss", scale(1.6), rotate_y(-30), translate(-0.5, 1.1, -0.6),
+          material_back="leaf", cutout="leafmask")
+    return s
+
 CONFIGS = {
     0: ("cornell", "Plain NEE+MIS Cornell box 256x256 16spp depth 8 seed 1"),
     1: ("instancing", "1024 icosphere-4 instances + 1024x512 env, 1920x1080 64spp"),

@@ -68,6 +68,23 @@ def test_cornell_parity(lib, oracle_lib):
     compare("cornell normal AOV", nrm + 2.0, on + 2.0)
 
 
+def test_cornell_config0_exact_parity(lib, oracle_lib):
+    """Config 0 at its own size: 256x256, 16 spp, max depth 8, seed 1, clamp 0."""
+    s = workloads.cornell(width=256, height=256, spp=16)
+    film, res, alb, nrm, of, orays, oa, on = render_both(s)
+    compare("cornell 256x256x16", film, of, res.rays_traced, orays)
+
+
+def test_image_textures_and_cutouts_parity(lib, oracle_lib, asset_dir):
+    """Image textures (sRGB and linear, bilinear with wrap), an image-textured
+    emitter sampled by NEE, and alpha cutouts on a quadric and on a uv-mapped
+    mesh, including shadow rays through the cutout holes."""
+    s = workloads.textured(asset_dir)
+    film, res, alb, nrm, of, orays, oa, on = render_both(s, base_dir=asset_dir)
+    compare("textured + cutouts", film, of, res.rays_traced, orays)
+    compare("textured albedo AOV", alb, oa)
+
+
 def test_features_parity(lib, oracle_lib):
     s = features_scene()
     film, res, alb, nrm, of, orays, oa, on = render_both(s)

@@ -46,12 +46,13 @@ def assert_same(name, ref, ours):
     assert not diff, "%s: %d lines differ, first %r" % (name, len(diff), diff[0])
 
 
-@pytest.mark.parametrize("which", ["cornell", "instancing", "volumes", "features"])
+@pytest.mark.parametrize("which", ["cornell", "instancing", "volumes", "features", "textured"])
 def test_workload_derivation_matches_reference(lib, asset_dir, which):
     s = {"cornell": lambda: workloads.cornell(),
          "instancing": lambda: workloads.instancing(asset_dir),
          "volumes": lambda: workloads.volumes(asset_dir),
-         "features": lambda: workloads.features()}[which]()
+         "features": lambda: workloads.features(),
+         "textured": lambda: workloads.textured(asset_dir)}[which]()
     ref, _ = oracle.reference_scene_text(s, asset_dir)
     h = s.build(asset_dir, lib)
     try:
