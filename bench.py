@@ -44,8 +44,24 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mrays/s"
 UNIT = "Mrays/s"
-WORKLOAD = ("instancing+env: 1024 fBm icosphere-4 instances (5.24M tris), 1024x512 HDR sky "
-            "+ sun, 1920x1080, 64 spp, depth 8, seed 1, clamp 0")
+WORKLOADS = {
+    0: ("cornell: 5 Lambert rects, emissive rect (17,12,4), GGX metal sphere r 0.3, glass "
+        "sphere ior 1.5; 256x256, 16 spp, depth 8, seed 1, clamp 0", (256, 256, 16)),
+    1: ("instancing+env: 1024 fBm icosphere-4 instances (5.24M tris), 1024x512 HDR sky "
+        "+ sun, 1920x1080, 64 spp, depth 8, seed 1, clamp 0", (1920, 1080, 64)),
+    2: ("volumes: 64-step flame with its point lights, water ior 1.33 with fBm normals and "
+        "Beer absorption, nested glass sphere, 5 rough glass panels, 2048-tri emissive mesh "
+        "light; 2560x1440, 256 spp, depth 8, seed 1, clamp 0", (2560, 1440, 256)),
+}
+# sundog's own gallery scenes that load no asset files, replayed from the call
+# streams its unchanged scenelib sends (tests/golden/abi_<scene>.json), with
+# the reference's published throughput at its benchmark settings (1920x1080,
+# 64 spp, the scene's own depth / clamp / seed; GB200, OptiX with software
+# traversal; reference docs/BENCHMARKS.md).
+GALLERY = {
+    "01-marble-run": (1209.0, "docs/BENCHMARKS.md:9"),
+    "02-cornell-lume": (819.0, "docs/BENCHMARKS.md:10"),
+}
 
 
 def parse_args():
@@ -54,9 +70,14 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--width", type=int, default=1920)
-    ap.add_argument("--height", type=int, default=1080)
-    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2],
+                    help="workload: 0 Cornell box, 1 instancing + env map (default), 2 volumes")
+    ap.add_argument("--scene", default=None, choices=sorted(GALLERY),
+                    help="instead of a config: one of sundog's gallery scenes at its "
+                         "published benchmark settings (1920x1080, 64 spp)")
+    ap.add_argument("--width", type=int, default=0, help="override the workload's width")
+    ap.add_argument("--height", type=int, default=0, help="override the workload's height")
+    ap.add_argument("--spp", type=int, default=0, help="override the workload's spp")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="target CPU time of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -90,9 +111,37 @@ def asset_dir():
     return d
 
 
+def resolve_workload(args):
+    """Fills args.width / height / spp from the workload and returns its
+    description and the reference's published Mrays/s for it (or None)."""
+    if args.scene:
+        w, h, spp = 1920, 1080, 64
+        desc = ("sundog gallery scene %s (its scenelib call stream replayed unchanged), "
+                "1920x1080, 64 spp, the scene's own depth, clamp and seed" % args.scene)
+        published = GALLERY[args.scene]
+    else:
+        desc, (w, h, spp) = WORKLOADS[args.config]
+        published = None
+    args.width = args.width or w
+    args.height = args.height or h
+    args.spp = args.spp or spp
+    if (args.width, args.height, args.spp) != (w, h, spp):
+        desc += " [overridden: %dx%d, %d spp]" % (args.width, args.height, args.spp)
+    return desc, published
+
+
 def make_scene(args):
+    if args.scene:
+        from sundog_b200 import callstream
+        return callstream.CallStreamScene(
+            os.path.join(ROOT, "tests", "golden", "abi_%s.json" % args.scene))
     from sundog_b200 import workloads
-    return workloads.instancing(asset_dir(), width=args.width, height=args.height, spp=args.spp)
+    make = {0: lambda: workloads.cornell(width=args.width, height=args.height, spp=args.spp),
+            1: lambda: workloads.instancing(asset_dir(), width=args.width, height=args.height,
+                                            spp=args.spp),
+            2: lambda: workloads.volumes(asset_dir(), width=args.width, height=args.height,
+                                         spp=args.spp)}
+    return make[args.config]()
 
 
 # ---- clocks ---------------------------------------------------------------------------
@@ -180,6 +229,74 @@ def bytes_per_ray(c):
     return total / max(c.rays, 1)
 
 
+def sum_counts(a, b):
+    """Both ray kinds' traversal counts together (the path loop's are a's)."""
+    from sundog_b200 import abi
+    c = abi.TraceCounts()
+    for f, _ in abi.TraceCounts._fields_:
+        setattr(c, f, getattr(a, f) + (0 if f.startswith("loop") else getattr(b, f)))
+    return c
+
+
+def profile_figures(name):
+    """`key: value` figures of a committed ncu summary under profiles/ (the
+    measured L2 bytes and issue-slot use of a kernel on a small case)."""
+    p = os.path.join(ROOT, "profiles", name)
+    out = {}
+    if os.path.isfile(p):
+        with open(p) as f:
+            for m in re.finditer(r"^([a-z0-9_]+):\s*([0-9.eE+-]+)\s*$", f.read(), re.M):
+                out[m.group(1)] = float(m.group(2))
+    return out
+
+
+def stage_roofline(lib, ses, stream, flush, rad, shd, peak, workload):
+    """One more render of the frame (after the timed steps, not part of
+    `value`) with per-stage CUDA events: each stage kernel's own time, and for
+    the two traversal stages their algorithmic bytes (radiance and shadow
+    rays counted apart) over that time. L2 bytes and issue-slot utilisation
+    come from the committed small-case ncu summary of the trace stage."""
+    import torch
+    from sundog_b200 import abi
+    abi.check(lib.sundog_session_set_stage_timing(ses.handle, 1), "stage timing", lib)
+    flush.fill_(1)
+    torch.cuda.synchronize()
+    ses.render(stream=stream.cuda_stream)
+    t = abi.StageTimes()
+    abi.check(lib.sundog_session_stage_times(ses.handle, ctypes.byref(t)), "stage times", lib)
+    abi.check(lib.sundog_session_set_stage_timing(ses.handle, 0), "stage timing", lib)
+    total = t.start_ms + t.trace_ms + t.shade_a_ms + t.shadow_ms + t.shade_b_ms
+    b_rad, b_shd = bytes_per_ray(rad), bytes_per_ray(shd)
+    out = {}
+    for name, ms, rays, bpr in (("wfTraceFetch", t.trace_ms, t.radiance_rays, b_rad),
+                                ("wfShadow", t.shadow_ms, t.shadow_rays, b_shd)):
+        ach = bpr * rays / (ms / 1e3) / 1e9 if ms > 0 else None
+        out[name] = {"ms_per_step": ms, "launches": t.iterations, "rays": rays,
+                     "mrays_per_s": rays / (ms / 1e3) / 1e6 if ms > 0 else None,
+                     "bytes_per_ray": bpr, "achieved_gbps": ach,
+                     "frac_of_hbm": ach / peak if ach else None,
+                     "share_of_stage_time": ms / total if total else None}
+    for name, ms in (("wfStart", t.start_ms), ("wfShadeA", t.shade_a_ms),
+                     ("wfShadeB", t.shade_b_ms)):
+        out[name] = {"ms_per_step": ms, "share_of_stage_time": ms / total if total else None}
+    prof = profile_figures("wf_trace_l2_issue_%s.md" % workload)
+    if prof:
+        tr = out["wfTraceFetch"]
+        if "l2_bytes_per_ray" in prof and tr["ms_per_step"]:
+            tr["l2_gbps"] = prof["l2_bytes_per_ray"] * tr["rays"] / (tr["ms_per_step"] / 1e3) / 1e9
+        for k in ("l2_bytes_per_ray", "l2_hit_rate_pct", "issue_slot_util_pct",
+                  "lanes_per_instruction", "l2_peak_gbps"):
+            if k in prof:
+                tr[k] = prof[k]
+        if "l2_gbps" in tr and "l2_peak_gbps" in prof:
+            tr["frac_of_l2"] = tr["l2_gbps"] / prof["l2_peak_gbps"]
+        tr["ncu_summary"] = "profiles/wf_trace_l2_issue_%s.md" % workload
+    out["iterations"] = t.iterations
+    out["note"] = ("per-stage CUDA events in one extra render after the timed steps; "
+                   "bytes per ray on a binary BVH, radiance and shadow rays counted apart")
+    return out
+
+
 # ---- CPU baseline (oracle on the host cores) ------------------------------------------
 
 def oracle_sample(scene, base_dir, args, seconds, threads):
@@ -187,7 +304,8 @@ def oracle_sample(scene, base_dir, args, seconds, threads):
     from oracle import oracle
     # The scene as sundog's own scene code derives it (oracle/_ref), so the
     # CPU arm loads nothing of this library.
-    text, r = oracle.reference_scene_text(scene, base_dir)
+    text, r = oracle.reference_scene_text(scene, base_dir, width=args.width, height=args.height,
+                                          spp=args.spp)
     osc = oracle.OracleScene(text)
     W, H, spp = r["width"], r["height"], r["spp"]
     # calibrate on one row
@@ -209,6 +327,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    desc, published = resolve_workload(args)
     scene = make_scene(args)
     threads = os.cpu_count() or 1
     per_step = max(2.0, min(args.cpu_seconds, 240.0 / max(args.steps + args.warmup, 1)))
@@ -225,9 +344,10 @@ def run_reference(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * t_all / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic" if not args.scene else "sundog gallery scene (recorded call stream)",
             "impl": "reference",
-            "config": {"workload": WORKLOAD, "width": args.width, "height": args.height,
+            "config": {"workload": desc, "width": args.width, "height": args.height,
                        "spp": args.spp},
             "cpu_baseline": last,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -280,12 +400,13 @@ def run_ours(args):
         build.build()
     lib = abi.load()
 
+    desc, published = resolve_workload(args)
     scene = make_scene(args)
     base = asset_dir()
     plan = shard_plan(rank, world, args.spp)
     fspp = plan["spp"]
     ses = sc.Session(scene, base_dir=base, engine=args.engine, shard_count=plan["shard_count"],
-                     shard_index=rank, spp=fspp)
+                     shard_index=rank, spp=fspp, width=args.width, height=args.height)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -342,7 +463,7 @@ def run_ours(args):
         h = scene.build(base, lib)
         try:
             film = np.zeros((args.height, args.width, 4), np.float32)
-            o = abi.options(quiet=True, spp=fspp)
+            o = abi.options(quiet=True, spp=fspp, width=args.width, height=args.height)
             ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, 0, 0, args.engine,
                                 plan["shard_count"], rank)
             rr = abi.RenderResult()
@@ -378,8 +499,10 @@ def run_ours(args):
     line = None
     if rank == 0:
         st = ses.stats
-        counts = abi.TraceCounts()
-        abi.check(lib.sundog_session_trace_counts(ses.handle, ctypes.byref(counts)), "counts", lib)
+        rad, shd = abi.TraceCounts(), abi.TraceCounts()
+        abi.check(lib.sundog_session_trace_counts_split(ses.handle, ctypes.byref(rad),
+                                                        ctypes.byref(shd)), "counts", lib)
+        counts = sum_counts(rad, shd)
         bpr = bytes_per_ray(counts)
         # Roofline unit: one chunk of samples (one persistent launch, or one
         # wavefront pass over the chunk's paths), timed by the session's events.
@@ -406,14 +529,24 @@ def run_ours(args):
                             "quadric, 64 B/instance) per chunk of samples (one persistent launch "
                             "or one wavefront pass) over its CUDA-event duration; the BVH (<4 MB) "
                             "and env tables are cache-resident, so HBM is a loose bound"}
+        if args.engine != 1:
+            roofline["per_kernel"] = stage_roofline(lib, ses, stream, flush, rad, shd, peak,
+                                                    args.scene or "config%d" % args.config)
         cpu = None
         if not args.no_cpu_baseline:
             cpu, _, _ = oracle_sample(scene, base, args, args.cpu_seconds, os.cpu_count() or 1)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "width": args.width, "height": args.height,
+                "scaling": "weak",
+                "vs_baseline": value / published[0] if published and world == 1 else None,
+                "published_reference": {"mrays_per_s": published[0], "source": published[1],
+                                        "hardware": "GB200 (no RT cores: OptiX software "
+                                                    "traversal), sundog's own build"}
+                if published else None,
+                "dtype": "f32", "data": "synthetic" if not args.scene else
+                "sundog gallery scene (recorded call stream)",
+                "config": {"workload": desc, "width": args.width, "height": args.height,
                            "spp": args.spp, "paths_per_step": int(paths_all / args.steps),
                            "l2": "flushed between steps (256 MiB write); BVH + env tables "
                                  "re-fetched each step",

@@ -291,6 +291,15 @@ SUNDOG_API int sundog_session_trace_counts_split(sundog_session*, sundog_trace_c
  * shade-A, shadow-ray and shade-B stages, the iterations, the radiance and
  * shadow rays traced and the stage launches. Megakernel renders leave it
  * zero. Returns 0/1. */
+/* A sampling table of the session's scene as the device holds it (no
+ * counterpart in the reference): which = 0 the environment's marginal CDF
+ * (H + 1 floats), 1 its conditional CDFs (H rows of W + 1 floats), 2 + k the
+ * area CDF of light k (triangles + 1 floats; empty unless light k is an
+ * emissive mesh). Copies min(cap, length) floats to out (may be NULL) and
+ * sets *count to the length. Returns 0/1. */
+SUNDOG_API int sundog_session_table(sundog_session*, int which, float* out, size_t cap,
+                                    size_t* count);
+
 typedef struct {
   double start_ms, trace_ms, shade_a_ms, shadow_ms, shade_b_ms;
   uint64_t iterations, radiance_rays, shadow_rays, launches;

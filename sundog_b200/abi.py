@@ -165,7 +165,7 @@ ADDITIVE_SYMBOLS = [
     "sundog_server_submit", "sundog_server_status", "sundog_server_wait",
     "sundog_server_cancel", "sundog_server_stats", "sundog_server_destroy",
     "sundog_session_copy_film", "sundog_session_trace_counts_split",
-    "sundog_session_set_stage_timing", "sundog_session_stage_times",
+    "sundog_session_set_stage_timing", "sundog_session_stage_times", "sundog_session_table",
 ]
 
 _lib = None
@@ -240,6 +240,8 @@ def load(path=None):
     lib.sundog_session_trace_counts.argtypes = [vp, ctypes.POINTER(TraceCounts)]
     lib.sundog_session_trace_counts_split.argtypes = [vp, ctypes.POINTER(TraceCounts),
                                                       ctypes.POINTER(TraceCounts)]
+    lib.sundog_session_table.argtypes = [vp, ip, vp, ctypes.c_size_t,
+                                         ctypes.POINTER(ctypes.c_size_t)]
     lib.sundog_session_set_stage_timing.argtypes = [vp, ip]
     lib.sundog_session_stage_times.argtypes = [vp, ctypes.POINTER(StageTimes)]
     lib.sundog_transfer_bytes.argtypes = [ctypes.POINTER(ctypes.c_uint64)] * 2

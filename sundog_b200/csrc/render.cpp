@@ -26,6 +26,7 @@
 #include "bvh_build.h"
 #include "guide.h"
 #include "kernels.h"
+#include "cdf_build.h"
 #include "render_session.h"
 #include "wavefront.h"
 #include "scene_model.h"
@@ -89,73 +90,6 @@ static void invertAffine(const Xform& x, float4 out[3]) {
     double tr = -(inv[r * 3] * t[0] + inv[r * 3 + 1] * t[1] + inv[r * 3 + 2] * t[2]);
     out[r] = make_float4((float)inv[r * 3], (float)inv[r * 3 + 1], (float)inv[r * 3 + 2], (float)tr);
   }
-}
-
-// Equirect CDFs over luminance * sin(theta), FP64 prefix sums stored as
-// float with the last entry pinned to 1; all-black rows get a uniform ramp.
-// (src/env_light.cpp:27-56) Rows are independent and run on several host
-// threads; the marginal prefix over the rows' sums stays sequential, so the
-// tables are bit-identical to a one-thread loop.
-void buildEnvCdf(const float* rgba, int w, int h, std::vector<float>& marg, std::vector<float>& cond,
-                 bool& degenerate) {
-  marg.assign(h + 1, 0.0f);
-  cond.assign((size_t)h * (w + 1), 0.0f);
-  std::vector<double> rowSum(h, 0.0);
-  auto rows = [&](int r0, int r1) {
-    for (int row = r0; row < r1; row++) {
-      float sinT = sinf(kPi * (row + 0.5f) / h);
-      float* cdf = &cond[(size_t)row * (w + 1)];
-      double sum = 0.0;
-      cdf[0] = 0.0f;
-      for (int col = 0; col < w; col++) {
-        const float* p = rgba + 4 * ((size_t)row * w + col);
-        float lum = 0.2126f * p[0] + 0.7152f * p[1] + 0.0722f * p[2];
-        sum += (double)(lum > 0.0f ? lum : 0.0f) * sinT;  // fmaxf(lum, 0), NaN -> 0
-        cdf[col + 1] = (float)sum;
-      }
-      if (sum > 0.0) {
-        for (int c = 1; c <= w; c++) cdf[c] = (float)(cdf[c] / sum);
-      } else {
-        for (int c = 0; c <= w; c++) cdf[c] = (float)c / w;
-      }
-      cdf[w] = 1.0f;
-      rowSum[row] = sum;
-    }
-  };
-  const int nt = std::max(1, std::min({8, (int)std::thread::hardware_concurrency(), h / 64}));
-  std::vector<std::thread> pool;
-  for (int t = 1; t < nt; t++) pool.emplace_back(rows, (int)((long)h * t / nt), (int)((long)h * (t + 1) / nt));
-  rows(0, h / nt);
-  for (std::thread& th : pool) th.join();
-  double total = 0.0;
-  for (int row = 0; row < h; row++) {
-    total += rowSum[row];
-    marg[row + 1] = (float)total;
-  }
-  degenerate = total <= 0.0;
-  if (!degenerate) {
-    for (int r = 1; r <= h; r++) marg[r] = (float)(marg[r] / total);
-  } else {
-    for (int r = 0; r <= h; r++) marg[r] = (float)r / h;
-  }
-  marg[h] = 1.0f;
-}
-
-// World-space triangle-area CDF of an emissive mesh instance: FP64 running
-// total, entries normalised once, last entry 1. (src/capi_render.cpp:143-155)
-void buildMeshLightCdf(const std::vector<float3>& wp, const std::vector<uint3>& idx,
-                       std::vector<float>& cdf, double& total) {
-  size_t n = idx.size();
-  cdf.assign(n + 1, 0.0f);
-  total = 0.0;
-  for (size_t t = 0; t < n; t++) {
-    const uint3& tr = idx[t];
-    total += 0.5 * (double)len(cross(wp[tr.y] - wp[tr.x], wp[tr.z] - wp[tr.x]));
-    cdf[t + 1] = (float)total;
-  }
-  if (!(total > 0.0)) return;
-  for (size_t t = 1; t < n; t++) cdf[t] = (float)(cdf[t] / total);
-  cdf[n] = 1.0f;
 }
 
 static int strataFor(int spp) {  // device/programs.cu:317-319
@@ -249,15 +183,16 @@ void DeviceScene::build(const SceneDesc& desc) {
   // ---- CDFs + BVH (the reference's "gas_build" segment) ----
   auto tBuild = Clock::now();
   if (scene.bgKind == BG_ENVMAP) {
-    std::vector<float> marg, cond;
+    // Texels up, then the CDFs built from them on the device (cdf_build.cu).
+    envTex.upload(envRgba.data(), envRgba.size() * sizeof(float));
+    envMarg.alloc((size_t)(envH + 1) * sizeof(float));
+    envCond.alloc((size_t)envH * (envW + 1) * sizeof(float));
     bool degenerate = false;
-    buildEnvCdf(envRgba.data(), envW, envH, marg, cond, degenerate);
+    buildEnvCdfDevice((const float4*)envTex.ptr, envW, envH, (float*)envMarg.ptr,
+                      (float*)envCond.ptr, degenerate, 0);
     if (degenerate && scene.env.importance)
       std::fprintf(stderr, "envmap: %s has zero luminance, falling back to uniform sampling\n",
                    scene.env.file.c_str());
-    envTex.upload(envRgba.data(), envRgba.size() * sizeof(float));
-    envMarg.upload(marg.data(), marg.size() * sizeof(float));
-    envCond.upload(cond.data(), cond.size() * sizeof(float));
     env.texels = (const float4*)envTex.ptr;
     env.margCdf = (const float*)envMarg.ptr;
     env.condCdf = (const float*)envCond.ptr;
@@ -285,23 +220,22 @@ void DeviceScene::build(const SceneDesc& desc) {
     meshDescs[i].numTris = (int)m.idx.size();
   }
 
-  // Mesh lights: render-local copy of the light list with world geometry.
-  std::vector<SdLight> lights = scene.lights;
+  // Mesh lights: render-local copy of the light list with world geometry;
+  // world vertices and area CDF built on the device (cdf_build.cu).
+  lights = scene.lights;
   for (const ObjectCfg& o : scene.objects) {
     if (o.kind != GK_MESH || o.lightId < 0) continue;
     const HostMesh& m = meshes[o.mesh];
-    std::vector<float3> wp(m.pos.size());
-    for (size_t i = 0; i < wp.size(); i++) wp[i] = o.xform.point(m.pos[i]);
-    std::vector<float> cdf;
-    double total = 0.0;
-    buildMeshLightCdf(wp, m.idx, cdf, total);
+    lightBufs.emplace_back();
+    lightBufs.back().alloc(m.pos.size() * sizeof(float3));
+    float3* dpos = (float3*)lightBufs.back().ptr;
+    lightBufs.emplace_back();
+    lightBufs.back().alloc((m.idx.size() + 1) * sizeof(float));
+    double total = buildMeshLightCdfDevice(meshDescs[o.mesh].pos, (int)m.pos.size(),
+                                           meshDescs[o.mesh].idx, (int)m.idx.size(), o.xform, dpos,
+                                           (float*)lightBufs.back().ptr, 0);
     if (!(total > 0.0))
       throw std::runtime_error("mesh NEE light has zero surface area: " + scene.meshes[o.mesh].file);
-    lightBufs.emplace_back();
-    lightBufs.back().upload(wp.data(), wp.size() * sizeof(float3));
-    const float3* dpos = (const float3*)lightBufs.back().ptr;
-    lightBufs.emplace_back();
-    lightBufs.back().upload(cdf.data(), cdf.size() * sizeof(float));
     SdLight& ld = lights[o.lightId];
     ld.mPos = dpos;
     ld.mCdf = (const float*)lightBufs.back().ptr;
@@ -434,6 +368,26 @@ void DeviceScene::build(const SceneDesc& desc) {
   cudaCheck(cudaDeviceSynchronize(), "scene upload");
   cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
   deviceBytes = freeBefore > freeB ? freeBefore - freeB : 0;
+}
+
+size_t DeviceScene::table(int which, float* out, size_t cap) const {
+  const float* src = nullptr;
+  size_t n = 0;
+  if (which == 0 && env.margCdf) {
+    src = env.margCdf;
+    n = (size_t)env.height + 1;
+  } else if (which == 1 && env.condCdf) {
+    src = env.condCdf;
+    n = (size_t)env.height * (env.width + 1);
+  } else if (which >= 2 && which - 2 < (int)lights.size() && lights[which - 2].mCdf) {
+    src = lights[which - 2].mCdf;
+    n = (size_t)lights[which - 2].mNumTris + 1;
+  } else if (which < 0) {
+    throw std::runtime_error("table: bad index");
+  }
+  if (out && src) cudaCheck(cudaMemcpy(out, src, std::min(n, cap) * sizeof(float),
+                                       cudaMemcpyDeviceToHost), "table download");
+  return n;
 }
 
 void DeviceScene::fillLaunch(SdLaunch& l) const {
@@ -863,6 +817,16 @@ extern "C" int sundog_session_trace_counts(sundog_session* sh, sundog_trace_coun
   SDB_TRY
   if (!sh || !out) throw std::runtime_error("session: null argument");
   reinterpret_cast<RenderSession*>(sh)->countTraversal(out);
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_session_table(sundog_session* sh, int which, float* out, size_t cap,
+                                    size_t* count) {
+  SDB_TRY
+  if (!sh) throw std::runtime_error("table: null session");
+  size_t n = reinterpret_cast<RenderSession*>(sh)->dev->table(which, out, cap);
+  if (count) *count = n;
   return SUNDOG_OK;
   SDB_CATCH(SUNDOG_ERROR)
 }

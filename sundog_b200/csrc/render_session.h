@@ -53,10 +53,6 @@ struct MeshBufs {
   DevBuf pos, idx, nrm, uv;
 };
 
-void buildEnvCdf(const float* rgba, int w, int h, std::vector<float>& marg, std::vector<float>& cond,
-                 bool& degenerate);
-void buildMeshLightCdf(const std::vector<float3>& wp, const std::vector<uint3>& idx,
-                       std::vector<float>& cdf, double& total);
 void quadricBoundsHost(int kind, float3& lo, float3& hi);
 
 struct GuideState;  // guide.h
@@ -78,8 +74,13 @@ struct DeviceScene {
   std::vector<MeshBufs> meshBufs;
   std::vector<DevBuf> lightBufs;
   DevBuf dNodes, dTris, dInst, dMeshes, dTex, dMat, dLights, dFlames;
+  std::vector<SdLight> lights;  // host copy of the device light list
 
   void build(const SceneDesc& desc);
+  // Copies sampling table `which` (0 env marginal CDF, 1 env conditional
+  // CDFs, 2 + k the area CDF of light k; empty when the scene has none) to
+  // out (cap floats); returns its length.
+  size_t table(int which, float* out, size_t cap) const;
   void fillLaunch(SdLaunch& l) const;  // scene pointers and counts
 };
 
