@@ -460,41 +460,53 @@ def run_ours(args):
     # download inside the timed call); whole job = slowest rank, summed rays.
     e2e = None
     if not args.no_e2e:
-        h = scene.build(base, lib)
-        try:
-            film = np.zeros((args.height, args.width, 4), np.float32)
-            o = abi.options(quiet=True, spp=fspp, width=args.width, height=args.height)
-            ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, 0, 0, args.engine,
-                                plan["shard_count"], rank)
-            rr = abi.RenderResult()
-            abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
-                                           ctypes.byref(rr)), "render_ex", lib)  # warm
-            h0, d0 = ctypes.c_uint64(), ctypes.c_uint64()
-            lib.sundog_transfer_bytes(ctypes.byref(h0), ctypes.byref(d0))
-            e_steps = max(1, min(args.steps, 3))
-            if dist:
-                dist.barrier()
-            t0 = time.perf_counter()
-            erays = 0
-            for _ in range(e_steps):
+        def e2e_run(keep):
+            """Calls of sundog_render_ex from the scene handle; keep = the
+            device-memory cache (off: every call allocates and frees all its
+            device buffers, the library's default)."""
+            abi.check(lib.sundog_set_device_memory_cache(1 if keep else 0), "cache", lib)
+            h = scene.build(base, lib)
+            try:
+                film = np.zeros((args.height, args.width, 4), np.float32)
+                o = abi.options(quiet=True, spp=fspp, width=args.width, height=args.height)
+                ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, 0, 0, args.engine,
+                                    plan["shard_count"], rank)
+                rr = abi.RenderResult()
                 abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
-                                               ctypes.byref(rr)), "render_ex", lib)
-                erays += rr.rays_traced
-            et = time.perf_counter() - t0
-            h1, d1 = ctypes.c_uint64(), ctypes.c_uint64()
-            lib.sundog_transfer_bytes(ctypes.byref(h1), ctypes.byref(d1))
-        finally:
-            lib.sundog_scene_destroy(h)
-        et, erays, hb, db = reduce_max_sum(dist, "cuda", et, erays, h1.value - h0.value,
-                                           d1.value - d0.value)
-        e2e = {"value": erays / et / 1e6, "unit": UNIT,
-               "h2d_bytes_per_step": int(hb / e_steps),
-               "d2h_bytes_per_step": int(db / e_steps),
-               "ms_per_step": 1000.0 * et / e_steps,
-               "last_call_ms": {"load": rr.load_ms, "build": rr.build_ms,
-                                "render": rr.render_ms, "total": rr.total_ms},
-               "path": "sundog_render_ex per rank: OBJ/HDR load, CDF + BVH build, upload, "
-                       "render, film download; slowest rank"}
+                                               ctypes.byref(rr)), "render_ex", lib)  # warm
+                h0, d0 = ctypes.c_uint64(), ctypes.c_uint64()
+                lib.sundog_transfer_bytes(ctypes.byref(h0), ctypes.byref(d0))
+                e_steps = max(1, min(args.steps, 3))
+                if dist:
+                    dist.barrier()
+                t0 = time.perf_counter()
+                erays = 0
+                for _ in range(e_steps):
+                    abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
+                                                   ctypes.byref(rr)), "render_ex", lib)
+                    erays += rr.rays_traced
+                et = time.perf_counter() - t0
+                h1, d1 = ctypes.c_uint64(), ctypes.c_uint64()
+                lib.sundog_transfer_bytes(ctypes.byref(h1), ctypes.byref(d1))
+            finally:
+                lib.sundog_scene_destroy(h)
+                abi.check(lib.sundog_set_device_memory_cache(0), "cache", lib)
+            et, erays, hb, db = reduce_max_sum(dist, "cuda", et, erays, h1.value - h0.value,
+                                               d1.value - d0.value)
+            return {"value": erays / et / 1e6, "unit": UNIT,
+                    "h2d_bytes_per_step": int(hb / e_steps),
+                    "d2h_bytes_per_step": int(db / e_steps),
+                    "ms_per_step": 1000.0 * et / e_steps,
+                    "last_call_ms": {"load": rr.load_ms, "build": rr.build_ms,
+                                     "render": rr.render_ms, "total": rr.total_ms}}
+        e2e = e2e_run(False)
+        e2e["path"] = ("sundog_render_ex per rank: OBJ/HDR load, CDF + BVH build, upload, "
+                       "render, film download, and every device buffer allocated and freed "
+                       "inside the call (the library's default); slowest rank")
+        cached = e2e_run(True)
+        e2e["with_memory_cache"] = {"value": cached["value"], "ms_per_step": cached["ms_per_step"],
+                                    "note": "sundog_set_device_memory_cache(1): the per-sample "
+                                            "buffer and path pool kept between calls"}
 
     line = None
     if rank == 0:

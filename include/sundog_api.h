@@ -291,6 +291,27 @@ SUNDOG_API int sundog_session_trace_counts_split(sundog_session*, sundog_trace_c
  * shade-A, shadow-ray and shade-B stages, the iterations, the radiance and
  * shadow rays traced and the stage launches. Megakernel renders leave it
  * zero. Returns 0/1. */
+/* The session's film as sundog's HDR output codes (no counterpart in the
+ * reference; src/film.cpp:96-115 computes the same codes on the host before
+ * its AVIF encode): x 2^exposure (exposure NaN = the scene's), BT.709 ->
+ * BT.2020, linear 1.0 at 203 cd/m^2, SMPTE ST 2084 PQ, 12-bit code, encoded
+ * on the device. out: width*height*3 uint16 (RGB, row 0 = top). sundog_render
+ * writes the same codes for a ".png" out_path (16-bit, cICP BT.2020/PQ), and
+ * for an ".avif" out_path beside it as ".png" (no AVIF encoder is linked).
+ * Returns 0/1. */
+SUNDOG_API int sundog_session_read_pq12(sundog_session*, double exposure, uint16_t* out);
+
+/* Device-memory cache between calls (no counterpart in the reference).
+ * Off by default: sundog_render / sundog_render_ex free every device buffer
+ * they allocated before returning, and a destroyed session frees its own.
+ * keep != 0: the per-sample radiance buffer (about 1 GiB) and the wavefront
+ * path pool of a finished render stay allocated on their device for the next
+ * render (saves their allocation and free per one-shot call) until
+ * sundog_release_device_memory() or sundog_set_device_memory_cache(0), which
+ * free them. Returns 0/1. */
+SUNDOG_API int sundog_set_device_memory_cache(int keep);
+SUNDOG_API int sundog_release_device_memory(void);
+
 /* A sampling table of the session's scene as the device holds it (no
  * counterpart in the reference): which = 0 the environment's marginal CDF
  * (H + 1 floats), 1 its conditional CDFs (H rows of W + 1 floats), 2 + k the

@@ -40,11 +40,50 @@ def pq_oetf(lin):
 
 
 def pq_codes12(film, exposure=0.0):
-    """12-bit PQ BT.2020 codes of a linear BT.709 film (H x W x >=3)."""
-    c = film[..., :3].astype(np.float32) * np.float32(2.0 ** exposure)
-    c = c @ BT709_TO_2020.T
-    e = pq_oetf(c * np.float32(PQ_WHITE_NITS / PQ_PEAK_NITS))
-    return np.floor(e * np.float32(4095.0) + np.float32(0.5)).astype(np.int32)
+    """12-bit PQ BT.2020 codes of a linear BT.709 film (H x W x >=3), each
+    FP32 operation in the reference's order (no fused multiply-adds)."""
+    f = np.float32
+    c = film[..., :3].astype(np.float32) * f(2.0 ** exposure)
+    x, y, z = c[..., 0], c[..., 1], c[..., 2]
+    m = BT709_TO_2020
+    rgb = np.stack([(m[r, 0] * x + m[r, 1] * y) + m[r, 2] * z for r in range(3)], -1)
+    e = pq_oetf(rgb * f(PQ_WHITE_NITS / PQ_PEAK_NITS)) * f(4095.0)
+    # lroundf: the FP32 value widened exactly to FP64, half away from zero.
+    return np.floor(e.astype(np.float64) + 0.5).astype(np.int32)
+
+
+def read_pq16_png(path):
+    """(codes, cicp) of a 16-bit RGB PNG written by the renderer: the 12-bit
+    codes (top 12 bits of each sample) as (H, W, 3) int32, and the cICP chunk
+    bytes (None if absent). Reads only what that writer emits: non-interlaced
+    RGB16 with filter type 0 rows."""
+    import struct
+    import zlib
+    with open(path, "rb") as fh:
+        data = fh.read()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n", "not a PNG"
+    return _read_png_chunks(data, struct, zlib)
+
+
+def _read_png_chunks(data, struct, zlib):
+    pos, idat, cicp, w, h = 8, b"", None, 0, 0
+    while pos < len(data):
+        n, = struct.unpack(">I", data[pos:pos + 4])
+        kind = data[pos + 4:pos + 8]
+        body = data[pos + 8:pos + 8 + n]
+        pos += 12 + n
+        if kind == b"IHDR":
+            w, h, depth, ctype = struct.unpack(">IIBB", body[:10])
+            assert depth == 16 and ctype == 2, "expected 16-bit RGB"
+        elif kind == b"cICP":
+            cicp = tuple(body)
+        elif kind == b"IDAT":
+            idat += body
+    raw = np.frombuffer(zlib.decompress(idat), np.uint8).reshape(h, 1 + w * 6)
+    assert np.all(raw[:, 0] == 0), "expected filter type 0 rows"
+    px = raw[:, 1:].reshape(h, w * 3, 2).astype(np.int32)
+    v = (px[..., 0] << 8) | px[..., 1]
+    return (v >> 4).reshape(h, w, 3), cicp
 
 
 def codes12_to_8(codes):

@@ -166,6 +166,7 @@ ADDITIVE_SYMBOLS = [
     "sundog_server_cancel", "sundog_server_stats", "sundog_server_destroy",
     "sundog_session_copy_film", "sundog_session_trace_counts_split",
     "sundog_session_set_stage_timing", "sundog_session_stage_times", "sundog_session_table",
+    "sundog_set_device_memory_cache", "sundog_release_device_memory", "sundog_session_read_pq12",
 ]
 
 _lib = None
@@ -242,6 +243,9 @@ def load(path=None):
                                                       ctypes.POINTER(TraceCounts)]
     lib.sundog_session_table.argtypes = [vp, ip, vp, ctypes.c_size_t,
                                          ctypes.POINTER(ctypes.c_size_t)]
+    lib.sundog_session_read_pq12.argtypes = [vp, dp, vp]
+    lib.sundog_set_device_memory_cache.argtypes = [ip]
+    lib.sundog_release_device_memory.argtypes = []
     lib.sundog_session_set_stage_timing.argtypes = [vp, ip]
     lib.sundog_session_stage_times.argtypes = [vp, ctypes.POINTER(StageTimes)]
     lib.sundog_transfer_bytes.argtypes = [ctypes.POINTER(ctypes.c_uint64)] * 2

@@ -22,7 +22,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 CU_SOURCES = ["pt_kernel.cu", "selftest.cu", "noalloc.cu", "guide.cu", "serve.cu", "wavefront.cu",
-              "cdf_build.cu"]
+              "cdf_build.cu", "film_out.cu"]
 CPP_SOURCES = ["scene_api.cpp", "scene_derive.cpp", "assets.cpp", "bvh_build.cpp",
                "render.cpp", "render_api.cpp", "serve_host.cpp"]
 
@@ -92,7 +92,8 @@ def build(verbose=False, force=False, defines=(), out=None):
                 print(out)
         objs.append(obj)
     link = [NVCC] + ARCH + ["-shared", "-o", lib_path] + objs + ["-cudart", "static", "-lpthread",
-                                                               "-Xlinker", "-soname=libsundog.so"]
+                                                               "-lz", "-Xlinker",
+                                                               "-soname=libsundog.so"]
     _run(link, verbose)
     return lib_path
 

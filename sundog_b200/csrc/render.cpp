@@ -52,6 +52,7 @@ void DevBuf::alloc(size_t n) {
   bytes = n;
 }
 std::atomic<unsigned long long> g_h2dBytes{0}, g_d2hBytes{0};
+void countDownload(size_t bytes) { g_d2hBytes += bytes; }
 
 void DevBuf::upload(const void* src, size_t n) {
   alloc(n);
@@ -99,11 +100,19 @@ static int strataFor(int spp) {  // device/programs.cu:317-319
   return n;
 }
 
-// One idle per-sample radiance buffer per device, kept between sessions: a
-// one-shot render (sundog_render, sundog_render_ex) would otherwise allocate
-// and free about 1 GiB per call (the free alone measured 5-60 ms).
+// Device-memory cache between calls (sundog_set_device_memory_cache): off by
+// default, so a one-shot render (sundog_render, sundog_render_ex) frees all
+// it allocated before it returns, as the reference's render does
+// (src/capi_render.cpp:65, 303-304). On, the largest per-sample radiance
+// buffer and the wavefront pool of a finished session stay allocated for the
+// next one on the same device (a one-shot render then skips allocating and
+// freeing about 1 GiB + the pool per call; the free alone measured 5-60 ms),
+// until sundog_release_device_memory or the cache is switched off.
+static std::atomic<int> g_keepMemory{0};
 static std::mutex g_samplesMu;
 static DevBuf g_idleSamples[64];
+
+bool keepDeviceMemory() { return g_keepMemory.load() != 0; }
 
 static void acquireSamples(DevBuf& b, size_t bytes) {
   int dev = 0;
@@ -121,8 +130,24 @@ static void acquireSamples(DevBuf& b, size_t bytes) {
 static void releaseSamples(DevBuf& b) {
   int dev = 0;
   if (!b.ptr || cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  if (!keepDeviceMemory()) {
+    b.release();
+    return;
+  }
   std::lock_guard<std::mutex> lock(g_samplesMu);
   if (g_idleSamples[dev].bytes < b.bytes) g_idleSamples[dev] = std::move(b);
+}
+
+// Frees the idle buffers of every device (the current device stays current).
+static void releaseIdleSamples() {
+  int cur = 0;
+  if (cudaGetDevice(&cur) != cudaSuccess) return;
+  std::lock_guard<std::mutex> lock(g_samplesMu);
+  for (int d = 0; d < 64; d++) {
+    if (!g_idleSamples[d].ptr) continue;
+    if (cudaSetDevice(d) == cudaSuccess) g_idleSamples[d].release();
+  }
+  cudaSetDevice(cur);
 }
 
 RenderSession::~RenderSession() {
@@ -817,6 +842,25 @@ extern "C" int sundog_session_trace_counts(sundog_session* sh, sundog_trace_coun
   SDB_TRY
   if (!sh || !out) throw std::runtime_error("session: null argument");
   reinterpret_cast<RenderSession*>(sh)->countTraversal(out);
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_set_device_memory_cache(int keep) {
+  SDB_TRY
+  g_keepMemory.store(keep ? 1 : 0);
+  if (!keep) {
+    releaseIdleSamples();
+    wfReleaseIdle();
+  }
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_release_device_memory(void) {
+  SDB_TRY
+  releaseIdleSamples();
+  wfReleaseIdle();
   return SUNDOG_OK;
   SDB_CATCH(SUNDOG_ERROR)
 }

@@ -3,9 +3,12 @@
 // src/capi_render.cpp:224-245 (stdout belongs to the calling program).
 //
 // Output: the reference encodes a 12-bit PQ BT.2020 AVIF through libavif
-// (src/film.cpp:96-115), which this build does not link. A ".pfm" or ".hdr"
-// out_path is written as linear float (exposure applied); any other
-// extension gets a ".pfm" file written beside it and a notice.
+// (src/film.cpp:96-115), which this build does not link. The same 12-bit PQ
+// codes are encoded on the device (film_out.cu) and written losslessly as a
+// 16-bit PNG with a BT.2020 / PQ cICP chunk: for a ".png" out_path there, for
+// an ".avif" out_path beside it (".png" replacing the extension) with a
+// notice. A ".pfm" or ".hdr" out_path is written as linear float (exposure
+// applied); any other extension gets a ".pfm" file beside it and a notice.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -17,6 +20,7 @@
 
 #include "../../include/sundog_api.h"
 #include "abi_util.h"
+#include "film_out.h"
 #include "guide.h"
 #include "render_session.h"
 #include "wavefront.h"
@@ -197,14 +201,26 @@ int renderImpl(sundog_scene* h, const sundog_render_options* opt, const sundog_r
   }
   float scale = exp2f(rs.exposure);
   if (opt->out_path && *opt->out_path) {
-    std::string wrote = writeImage(opt->out_path, film, rs.width, rs.height, scale);
+    std::string out = opt->out_path, wrote;
+    const bool avif = endsWith(out, ".avif");
+    if (avif || endsWith(out, ".png")) {
+      if (avif) out = out.substr(0, out.size() - 5) + ".png";
+      std::vector<unsigned short> codes(npix * 3);
+      encodePq12((const float4*)s->accum.ptr, rs.width, rs.height, rs.exposure, codes.data(),
+                 s->stream);
+      writePq16Png(out, codes.data(), rs.width, rs.height);
+      wrote = out;
+    } else {
+      wrote = writeImage(opt->out_path, film, rs.width, rs.height, scale);
+    }
     if (opt->aov_albedo_path) writeImage(opt->aov_albedo_path, alb.data(), rs.width, rs.height, 1.0f);
     if (opt->aov_normal_path) writeImage(opt->aov_normal_path, nrm.data(), rs.width, rs.height, 1.0f);
     if (!quiet) {
       std::fprintf(stderr, "Rendering elapsed time: %f seconds (%.0f Mrays/s)\nwrote %s\n",
                    r.render_ms / 1000.0, r.mrays_per_sec, wrote.c_str());
       if (wrote != opt->out_path)
-        std::fprintf(stderr, "sundog: AVIF output needs libavif; wrote linear PFM instead\n");
+        std::fprintf(stderr, "sundog: no AVIF encoder in this build; wrote %s instead\n",
+                     wrote.c_str());
     }
   }
   size_t freeAfter = 0, tot = 0;
@@ -220,6 +236,17 @@ int renderImpl(sundog_scene* h, const sundog_render_options* opt, const sundog_r
 }
 
 }  // namespace
+
+extern "C" int sundog_session_read_pq12(sundog_session* sh, double exposure, uint16_t* out) {
+  SDB_TRY
+  if (!sh || !out) throw std::runtime_error("read pq12: null argument");
+  RenderSession& s = *reinterpret_cast<RenderSession*>(sh);
+  float ev = std::isnan(exposure) ? s.scene.render.exposure : (float)exposure;
+  encodePq12((const float4*)s.accum.ptr, s.lp.width, s.lp.height, ev, out, s.stream);
+  countDownload((size_t)s.lp.width * s.lp.height * 3 * sizeof(uint16_t));
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
 
 // src/capi_render.cpp:280-307
 extern "C" int sundog_render(sundog_scene* h, const sundog_render_options* opt) {

@@ -13,6 +13,8 @@
 namespace sdb {
 
 void cudaCheck(cudaError_t e, const char* what);
+// Adds to the device-to-host byte count sundog_transfer_bytes reports.
+void countDownload(size_t bytes);
 
 // Per-stage device time of wavefront renders, accumulated while a session
 // has stage timing on: CUDA events on the render stream around each stage

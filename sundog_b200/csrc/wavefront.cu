@@ -622,9 +622,9 @@ WfBuffers::~WfBuffers() {
     if (e) cudaEventDestroy(e);
 }
 
-// One idle pool per device, kept between sessions: a one-shot render
-// (sundog_render, sundog_render_ex) would otherwise allocate and free 1.3 GB
-// of slots per call.
+// One idle pool per device, kept between sessions while the device-memory
+// cache is on (sundog_set_device_memory_cache); otherwise a finished
+// session's pool is freed with it.
 static std::mutex g_poolMu;
 static std::unique_ptr<WfBuffers> g_idle[64];
 
@@ -640,8 +640,20 @@ void wfRelease(std::unique_ptr<WfBuffers> b) {
   if (!b) return;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  if (!keepDeviceMemory()) return;  // b frees its buffers here
   std::lock_guard<std::mutex> lock(g_poolMu);
   if (!g_idle[dev] || g_idle[dev]->cap < b->cap) g_idle[dev] = std::move(b);
+}
+
+void wfReleaseIdle() {
+  int cur = 0;
+  if (cudaGetDevice(&cur) != cudaSuccess) return;
+  std::lock_guard<std::mutex> lock(g_poolMu);
+  for (int d = 0; d < 64; d++) {
+    if (!g_idle[d]) continue;
+    if (cudaSetDevice(d) == cudaSuccess) g_idle[d].reset();
+  }
+  cudaSetDevice(cur);
 }
 
 size_t wfSlotBytes() {

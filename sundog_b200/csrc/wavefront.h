@@ -64,6 +64,11 @@ size_t wfSlotBytes();
 // or a new empty one. wfRelease keeps a finished session's pool for reuse.
 std::unique_ptr<WfBuffers> wfAcquire();
 void wfRelease(std::unique_ptr<WfBuffers> b);
+// Frees the idle pools of every device.
+void wfReleaseIdle();
+// Whether finished sessions keep their device buffers for the next one
+// (sundog_set_device_memory_cache; render.cpp).
+bool keepDeviceMemory();
 // Renders lp.numPaths camera paths (counters cleared by the caller) into
 // lp.sampleL; returns the number of kernels launched. Synchronises st once per
 // iteration to read the live-path count. guide: 0, or a combination of

@@ -1,0 +1,67 @@
+"""HDR output: the film's 12-bit PQ BT.2020 codes encoded on the device
+(sundog_session_read_pq12, and the 16-bit PNG sundog_render writes for a
+.png or .avif out_path) against the oracle's restatement of sundog's host
+encode (oracle/film_pq.py; src/film.cpp:96-115, src/transfer.h).
+
+Bound: the encode is a per-pixel chain of FP32 operations in the reference's
+order plus two powf calls, whose device and host implementations may differ
+by an ulp; a code can then move by one where the value sits at a half-code
+boundary. >= 99.9% of codes identical, none off by more than 1."""
+
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from oracle import film_pq
+from sundog_b200 import abi, workloads
+from sundog_b200 import scene as sc
+
+pytestmark = pytest.mark.gpu
+
+
+def compare_codes(name, got, ref):
+    got = np.asarray(got, np.int64)
+    ref = np.asarray(ref, np.int64)
+    d = np.abs(got - ref)
+    same = np.mean(d == 0)
+    print("%-24s codes identical %.6f  max diff %d  range %d..%d"
+          % (name, same, d.max(), ref.min(), ref.max()))
+    assert same >= 0.999, name
+    assert d.max() <= 1, name
+
+
+def test_pq12_codes_match_reference_encode(lib):
+    s = workloads.features()
+    for ev in (0.0, 1.5, -2.0):
+        with sc.Session(s) as ses:
+            ses.render()
+            film = ses.read()
+            st = ses.stats
+            codes = np.zeros((st.height, st.width, 3), np.uint16)
+            abi.check(lib.sundog_session_read_pq12(ses.handle, ev, codes.ctypes.data), "pq12",
+                      lib)
+        compare_codes("features EV %+.1f" % ev, codes, film_pq.pq_codes12(film, ev))
+    # bright and dark extremes reach both ends of the code range
+    assert codes.max() > 3000 and codes.min() < 200
+
+
+def test_render_writes_pq_png(lib, tmp_path):
+    s = workloads.cornell(width=48, height=40, spp=4)
+    h = s.build(".", lib)
+    try:
+        out = str(tmp_path / "frame.avif")
+        film = np.zeros((40, 48, 4), np.float32)
+        o = abi.options(out=out, quiet=True)
+        ext = abi.RenderExt(film.ctypes.data, None, None, 0, 1, 0, 0, 0, 0)
+        res = abi.RenderResult()
+        abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext), ctypes.byref(res)),
+                  "render", lib)
+    finally:
+        lib.sundog_scene_destroy(h)
+    png = str(tmp_path / "frame.png")
+    assert os.path.isfile(png) and not os.path.exists(out)
+    codes, cicp = film_pq.read_pq16_png(png)
+    assert cicp == (9, 16, 0, 1)
+    compare_codes("cornell PNG", codes, film_pq.pq_codes12(film))
