@@ -301,6 +301,13 @@ SUNDOG_API int sundog_session_trace_counts_split(sundog_session*, sundog_trace_c
  * Returns 0/1. */
 SUNDOG_API int sundog_session_read_pq12(sundog_session*, double exposure, uint16_t* out);
 
+/* Which builder makes the binary BVHs of later scene uploads (no counterpart
+ * in the reference, whose optixAccelBuild runs on the device,
+ * src/accel.cpp:46-121): device != 0 (the default) builds every mesh's BVH and
+ * the instance BVH on the GPU; 0 uses the host binned-SAH builder. Both apply
+ * the same split rules; the trees differ only in tie-breaking. Returns 0/1. */
+SUNDOG_API int sundog_set_bvh_builder(int device);
+
 /* Device-memory cache between calls (no counterpart in the reference).
  * Off by default: sundog_render / sundog_render_ex free every device buffer
  * they allocated before returning, and a destroyed session frees its own.

@@ -22,7 +22,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 CU_SOURCES = ["pt_kernel.cu", "selftest.cu", "noalloc.cu", "guide.cu", "serve.cu", "wavefront.cu",
-              "cdf_build.cu", "film_out.cu"]
+              "cdf_build.cu", "film_out.cu", "bvh_device.cu"]
 CPP_SOURCES = ["scene_api.cpp", "scene_derive.cpp", "assets.cpp", "bvh_build.cpp",
                "render.cpp", "render_api.cpp", "serve_host.cpp"]
 
@@ -68,14 +68,15 @@ def _run(cmd, verbose):
 
 
 def build(verbose=False, force=False, defines=(), out=None):
-    """Compile every translation unit (cached by content hash) and link.
-    `defines` adds -D flags to every unit (tuning experiments); `out`
-    overrides the output library path."""
+    """Compile every translation unit (cached by content hash, in parallel)
+    and link. `defines` adds -D flags to every unit; `out` overrides the
+    output library path."""
+    from concurrent.futures import ThreadPoolExecutor
     lib_path = out or LIB
     os.makedirs(os.path.dirname(lib_path), exist_ok=True)
     os.makedirs(OBJ_DIR, exist_ok=True)
     hdr = _headers_digest()
-    objs = []
+    objs, jobs = [], []
     for src in _sources():
         path = os.path.join(CSRC, src)
         is_cu = src.endswith(".cu")
@@ -84,13 +85,15 @@ def build(verbose=False, force=False, defines=(), out=None):
         obj = os.path.join(OBJ_DIR, "%s.%s.o" % (src, tag))
         if force or not os.path.exists(obj):
             if is_cu:
-                cmd = [NVCC] + flags + ["-c", path, "-o", obj]
+                jobs.append([NVCC] + flags + ["-c", path, "-o", obj])
             else:
-                cmd = ["g++"] + flags + ["-c", path, "-o", obj]
-            out = _run(cmd, verbose)
-            if verbose and out.strip():
-                print(out)
+                jobs.append(["g++"] + flags + ["-c", path, "-o", obj])
         objs.append(obj)
+    if jobs:
+        with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+            for text in ex.map(lambda c: _run(c, verbose), jobs):
+                if verbose and text.strip():
+                    print(text)
     link = [NVCC] + ARCH + ["-shared", "-o", lib_path] + objs + ["-cudart", "static", "-lpthread",
                                                                "-lz", "-Xlinker",
                                                                "-soname=libsundog.so"]
@@ -98,5 +101,19 @@ def build(verbose=False, force=False, defines=(), out=None):
     return lib_path
 
 
+# The same sources with the compressed 8-wide BVH (8-bit outward-rounded child
+# boxes, SDB_WIDE_BVH) in place of the binary one: a second in-tree library
+# with the identical ABI, loaded instead of the default through the
+# SUNDOG_B200_LIB environment variable.
+LIB_CW8 = os.path.join(OUT_DIR, "libsundog_cw8.so")
+
+
+def build_all(verbose=False, force=False):
+    """Both libraries: the default (binary BVH) and the 8-wide variant."""
+    build(verbose=verbose, force=force)
+    build(verbose=verbose, force=force, defines=("SDB_WIDE_BVH=1",), out=LIB_CW8)
+    return LIB, LIB_CW8
+
+
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))
+    print(build_all(verbose="-v" in sys.argv, force="-f" in sys.argv))

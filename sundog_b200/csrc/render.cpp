@@ -24,6 +24,7 @@
 #include "abi_util.h"
 #include "assets.h"
 #include "bvh_build.h"
+#include "bvh_device.h"
 #include "guide.h"
 #include "kernels.h"
 #include "cdf_build.h"
@@ -272,81 +273,89 @@ void DeviceScene::build(const SceneDesc& desc) {
                             o.xform.vec(v3(0, 0, 1)));
   }
 
-  // BLAS per mesh, TLAS over objects: compressed 8-wide trees in one array
-  // (TLAS first), triangles stored in leaf order.
-  std::vector<float4> allTris;
+  // BLAS per mesh, TLAS over objects, in one node array (TLAS first);
+  // triangles stored in leaf order. The binary layout is built on the device
+  // (bvh_device.cu) unless the host builder is selected
+  // (sundog_set_bvh_builder); the 8-wide layout is built on the host.
   int nObj = (int)scene.objects.size();
-  std::vector<Box3> instBoxes(nObj);
-  for (int i = 0; i < nObj; i++) {
-    const ObjectCfg& o = scene.objects[i];
-    Box3 b = boxEmpty();
-    if (o.kind == GK_MESH) {
-      for (const float3& p : meshes[o.mesh].pos) boxGrow(b, o.xform.point(p));
-    } else {
-      float3 lo, hi;
-      quadricBoundsHost(o.kind, lo, hi);
-      for (int c = 0; c < 8; c++)
-        boxGrow(b, o.xform.point(v3(c & 1 ? hi.x : lo.x, c & 2 ? hi.y : lo.y, c & 4 ? hi.z : lo.z)));
-    }
-    // World boxes come from rounded corner transforms: pad by a few ulps.
-    float3 pad = (vmax(vmax(b.hi, -b.hi), vmax(b.lo, -b.lo)) + v3(1.0f)) * 1e-6f;
-    b.lo = b.lo - pad;
-    b.hi = b.hi + pad;
-    instBoxes[i] = b;
-  }
-  // Kernel-matched layout: binary nodes, or compressed 8-wide nodes.
   const bool wide = bvhWidth() == 8;
+  std::vector<int> tlasOrder;
+  bool builtOnDevice = false;
+  if (!wide && nObj > 0 && deviceBvhBuilds()) {
+    buildAccelOnDevice(meshes, meshDescs, tlasOrder);
+    builtOnDevice = true;
+  }
+  std::vector<float4> allTris;
   std::vector<CwNode> cwNodes;
   std::vector<BvhNode> binNodes;
-  std::vector<int> tlasOrder;
-  if (wide) {
-    CwBuild tlas = buildCw(instBoxes, 1, 0, 0);
-    cwNodes = tlas.nodes;
-    tlasOrder = tlas.order;
-    tlasDepth = tlas.maxDepth;
-  } else {
-    BvhBuild tlas = buildBvh(instBoxes, 1, 0, 0);
-    binNodes = tlas.nodes;
-    tlasOrder = tlas.order;
-    tlasDepth = tlas.maxDepth;
-  }
-  blasDepth = 0;
-  for (size_t i = 0; i < meshes.size(); i++) {
-    const HostMesh& m = meshes[i];
-    std::vector<Box3> tb(m.idx.size());
-    for (size_t t = 0; t < m.idx.size(); t++) {
+  if (!builtOnDevice) {
+    std::vector<Box3> instBoxes(nObj);
+    for (int i = 0; i < nObj; i++) {
+      const ObjectCfg& o = scene.objects[i];
       Box3 b = boxEmpty();
-      boxGrow(b, m.pos[m.idx[t].x]);
-      boxGrow(b, m.pos[m.idx[t].y]);
-      boxGrow(b, m.pos[m.idx[t].z]);
-      tb[t] = b;
+      if (o.kind == GK_MESH) {
+        for (const float3& p : meshes[o.mesh].pos) boxGrow(b, o.xform.point(p));
+      } else {
+        float3 lo, hi;
+        quadricBoundsHost(o.kind, lo, hi);
+        for (int c = 0; c < 8; c++)
+          boxGrow(b, o.xform.point(v3(c & 1 ? hi.x : lo.x, c & 2 ? hi.y : lo.y, c & 4 ? hi.z : lo.z)));
+      }
+      // World boxes come from rounded corner transforms: pad by a few ulps.
+      float3 pad = (vmax(vmax(b.hi, -b.hi), vmax(b.lo, -b.lo)) + v3(1.0f)) * 1e-6f;
+      b.lo = b.lo - pad;
+      b.hi = b.hi + pad;
+      instBoxes[i] = b;
     }
-    int primBase = (int)(allTris.size() / 3);
-    std::vector<int> order;
     if (wide) {
-      int nodeBase = (int)cwNodes.size();
-      CwBuild bl = buildCw(tb, kCwLeafMax, nodeBase, primBase);
-      blasDepth = std::max(blasDepth, bl.maxDepth);
-      meshDescs[i].root = nodeBase;
-      cwNodes.insert(cwNodes.end(), bl.nodes.begin(), bl.nodes.end());
-      order = bl.order;
+      CwBuild tlas = buildCw(instBoxes, 1, 0, 0);
+      cwNodes = tlas.nodes;
+      tlasOrder = tlas.order;
+      tlasDepth = tlas.maxDepth;
     } else {
-      int nodeBase = (int)binNodes.size();
-      BvhBuild bl = buildBvh(tb, 4, nodeBase, primBase);
-      blasDepth = std::max(blasDepth, bl.maxDepth);
-      meshDescs[i].root = nodeBase;
-      binNodes.insert(binNodes.end(), bl.nodes.begin(), bl.nodes.end());
-      order = bl.order;
+      BvhBuild tlas = buildBvh(instBoxes, 1, 0, 0);
+      binNodes = tlas.nodes;
+      tlasOrder = tlas.order;
+      tlasDepth = tlas.maxDepth;
     }
-    for (int k : order) {
-      const uint3& t = m.idx[k];
-      float3 a = m.pos[t.x], b = m.pos[t.y], c = m.pos[t.z];
-      int ki = k;
-      float kf;
-      std::memcpy(&kf, &ki, sizeof kf);
-      allTris.push_back(make_float4(a.x, a.y, a.z, kf));
-      allTris.push_back(make_float4(b.x, b.y, b.z, 0.0f));
-      allTris.push_back(make_float4(c.x, c.y, c.z, 0.0f));
+    blasDepth = 0;
+    for (size_t i = 0; i < meshes.size(); i++) {
+      const HostMesh& m = meshes[i];
+      std::vector<Box3> tb(m.idx.size());
+      for (size_t t = 0; t < m.idx.size(); t++) {
+        Box3 b = boxEmpty();
+        boxGrow(b, m.pos[m.idx[t].x]);
+        boxGrow(b, m.pos[m.idx[t].y]);
+        boxGrow(b, m.pos[m.idx[t].z]);
+        tb[t] = b;
+      }
+      int primBase = (int)(allTris.size() / 3);
+      std::vector<int> order;
+      if (wide) {
+        int nodeBase = (int)cwNodes.size();
+        CwBuild bl = buildCw(tb, kCwLeafMax, nodeBase, primBase);
+        blasDepth = std::max(blasDepth, bl.maxDepth);
+        meshDescs[i].root = nodeBase;
+        cwNodes.insert(cwNodes.end(), bl.nodes.begin(), bl.nodes.end());
+        order = bl.order;
+      } else {
+        int nodeBase = (int)binNodes.size();
+        BvhBuild bl = buildBvh(tb, 4, nodeBase, primBase);
+        blasDepth = std::max(blasDepth, bl.maxDepth);
+        meshDescs[i].root = nodeBase;
+        binNodes.insert(binNodes.end(), bl.nodes.begin(), bl.nodes.end());
+        order = bl.order;
+      }
+      for (int k : order) {
+        const uint3& t = m.idx[k];
+        float3 a = m.pos[t.x], b = m.pos[t.y], c = m.pos[t.z];
+        int ki = k;
+        float kf;
+        std::memcpy(&kf, &ki, sizeof kf);
+        allTris.push_back(make_float4(a.x, a.y, a.z, kf));
+        allTris.push_back(make_float4(b.x, b.y, b.z, 0.0f));
+        allTris.push_back(make_float4(c.x, c.y, c.z, 0.0f));
+      }
     }
   }
   // A traversal keeps at most one stack entry per tree level (plus its
@@ -373,13 +382,15 @@ void DeviceScene::build(const SceneDesc& desc) {
     bool trans = matTransmissive(scene, o.matFront) || matTransmissive(scene, o.matBack);
     in.flags = (masked ? kInstMasked : 0) | (trans ? kInstTransmissive : 0);
   }
-  numNodes = wide ? cwNodes.size() : binNodes.size();
-  numTris = allTris.size() / 3;
-  if (wide)
-    dNodes.upload(cwNodes.data(), cwNodes.size() * sizeof(CwNode));
-  else
-    dNodes.upload(binNodes.data(), binNodes.size() * sizeof(BvhNode));
-  dTris.upload(allTris.data(), allTris.size() * sizeof(float4));
+  if (!builtOnDevice) {
+    numNodes = wide ? cwNodes.size() : binNodes.size();
+    numTris = allTris.size() / 3;
+    if (wide)
+      dNodes.upload(cwNodes.data(), cwNodes.size() * sizeof(CwNode));
+    else
+      dNodes.upload(binNodes.data(), binNodes.size() * sizeof(BvhNode));
+    dTris.upload(allTris.data(), allTris.size() * sizeof(float4));
+  }
   dInst.upload(inst.data(), inst.size() * sizeof(SdInstance));
   dMeshes.upload(meshDescs.data(), meshDescs.size() * sizeof(SdMesh));
   dTex.upload(texDescs.data(), texDescs.size() * sizeof(SdTexture));
@@ -393,6 +404,133 @@ void DeviceScene::build(const SceneDesc& desc) {
   cudaCheck(cudaDeviceSynchronize(), "scene upload");
   cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
   deviceBytes = freeBefore > freeB ? freeBefore - freeB : 0;
+}
+
+// Which builder makes the binary BVH (sundog_set_bvh_builder): 1 = on the
+// device (default), 0 = the host binned-SAH builder.
+static std::atomic<int> g_deviceBvh{1};
+bool deviceBvhBuilds() { return g_deviceBvh.load() != 0; }
+
+namespace {
+// One node whose first child is a leaf holding all n primitives and whose
+// second is an empty box far away (never entered): the root of a tree too
+// small to split, as the host builder makes it.
+BvhNode singleLeafRoot(const Box3& b, int link) {
+  BvhNode nd;
+  nd.xy0 = make_float4(b.lo.x, b.hi.x, b.lo.y, b.hi.y);
+  nd.xy1 = make_float4(3e30f, 3e30f, 3e30f, 3e30f);
+  nd.zz = make_float4(b.lo.z, b.hi.z, 3e30f, 3e30f);
+  nd.link = make_int4(link, link, 0, 0);
+  return nd;
+}
+}  // namespace
+
+void DeviceScene::buildAccelOnDevice(const std::vector<HostMesh>& meshes,
+                                     std::vector<SdMesh>& meshDescs,
+                                     std::vector<int>& tlasOrder) {
+  const int nObj = (int)scene.objects.size();
+  cudaStream_t st = 0;
+  // Node capacity: at most n - 1 inner nodes per tree of n > 1 primitives.
+  size_t cap = (size_t)std::max(nObj - 1, 1);
+  size_t totalTris = 0;
+  for (const HostMesh& m : meshes) {
+    cap += (size_t)std::max((int)m.idx.size() - 1, 1);
+    totalTris += m.idx.size();
+  }
+  dNodes.alloc(cap * sizeof(BvhNode));
+  dTris.alloc(std::max<size_t>(totalTris, 1) * 3 * sizeof(float4));
+  BvhNode* nodes = (BvhNode*)dNodes.ptr;
+  float4* tris = (float4*)dTris.ptr;
+
+  // TLAS over the instances' world boxes.
+  std::vector<DevInstanceSrc> src(nObj);
+  for (int i = 0; i < nObj; i++) {
+    const ObjectCfg& o = scene.objects[i];
+    DevInstanceSrc& d = src[i];
+    std::memset(&d, 0, sizeof d);
+    std::memcpy(d.xf, o.xform.m, sizeof d.xf);
+    if (o.kind == GK_MESH) {
+      d.pos = meshDescs[o.mesh].pos;
+      d.numVerts = (int)meshes[o.mesh].pos.size();
+    } else {
+      quadricBoundsHost(o.kind, d.qlo, d.qhi);
+    }
+  }
+  DevBuf dSrc, boxLo, boxHi, cent, order;
+  dSrc.upload(src.data(), src.size() * sizeof(DevInstanceSrc));
+  size_t maxPrims = std::max<size_t>((size_t)nObj, 1);
+  for (const HostMesh& m : meshes) maxPrims = std::max(maxPrims, m.idx.size());
+  boxLo.alloc(maxPrims * sizeof(float4));
+  boxHi.alloc(maxPrims * sizeof(float4));
+  cent.alloc(maxPrims * sizeof(float4));
+  order.alloc(maxPrims * sizeof(int));
+  instanceBoxesDevice((const DevInstanceSrc*)dSrc.ptr, nObj, (float4*)boxLo.ptr,
+                      (float4*)boxHi.ptr, (float4*)cent.ptr, st);
+  int cursor = 0;
+  tlasOrder.assign(nObj, 0);
+  if (nObj > 1) {
+    DevBvhStats t = buildBvhDevice((const float4*)boxLo.ptr, (const float4*)boxHi.ptr,
+                                   (const float4*)cent.ptr, nObj, 1, 0, 0, nodes, nObj - 1,
+                                   (int*)order.ptr, st);
+    cudaCheck(cudaMemcpy(tlasOrder.data(), order.ptr, nObj * sizeof(int), cudaMemcpyDeviceToHost),
+              "TLAS order");
+    tlasDepth = t.maxDepth;
+    cursor = t.nodes;
+  } else {
+    float4 l, h;
+    cudaCheck(cudaMemcpy(&l, boxLo.ptr, sizeof l, cudaMemcpyDeviceToHost), "instance box");
+    cudaCheck(cudaMemcpy(&h, boxHi.ptr, sizeof h, cudaMemcpyDeviceToHost), "instance box");
+    BvhNode root = singleLeafRoot({v3(l.x, l.y, l.z), v3(h.x, h.y, h.z)}, ~0);
+    cudaCheck(cudaMemcpy(nodes, &root, sizeof root, cudaMemcpyHostToDevice), "TLAS root");
+    tlasDepth = 0;
+    cursor = 1;
+  }
+
+  // One BLAS per mesh (leaves of up to 4 triangles), triangles gathered into
+  // leaf order after each build.
+  blasDepth = 0;
+  int triCursor = 0;
+  for (size_t i = 0; i < meshes.size(); i++) {
+    const HostMesh& m = meshes[i];
+    const int nt = (int)m.idx.size();
+    meshDescs[i].root = cursor;
+    if (nt > 4) {
+      meshBoxesDevice(meshDescs[i].pos, meshDescs[i].idx, nt, (float4*)boxLo.ptr,
+                      (float4*)boxHi.ptr, (float4*)cent.ptr, st);
+      DevBvhStats b = buildBvhDevice((const float4*)boxLo.ptr, (const float4*)boxHi.ptr,
+                                     (const float4*)cent.ptr, nt, 4, cursor, triCursor,
+                                     nodes + cursor, nt - 1, (int*)order.ptr, st);
+      blasDepth = std::max(blasDepth, b.maxDepth);
+      gatherTrisDevice(meshDescs[i].pos, meshDescs[i].idx, (const int*)order.ptr, nt,
+                       tris + 3 * (size_t)triCursor, st);
+      cursor += b.nodes;
+    } else {
+      // Too small to split: one leaf under a single root node.
+      Box3 b = boxEmpty();
+      std::vector<int> ident(std::max(nt, 1));
+      for (int t = 0; t < nt; t++) {
+        ident[t] = t;
+        boxGrow(b, m.pos[m.idx[t].x]);
+        boxGrow(b, m.pos[m.idx[t].y]);
+        boxGrow(b, m.pos[m.idx[t].z]);
+      }
+      int link = nt > 0 ? ~((triCursor << 3) | (nt - 1)) : ~0;
+      BvhNode root = nt > 0 ? singleLeafRoot(b, link)
+                            : singleLeafRoot({v3(3e30f), v3(3e30f)}, ~0);
+      cudaCheck(cudaMemcpy(nodes + cursor, &root, sizeof root, cudaMemcpyHostToDevice), "BLAS root");
+      if (nt > 0) {
+        cudaCheck(cudaMemcpy(order.ptr, ident.data(), nt * sizeof(int), cudaMemcpyHostToDevice),
+                  "BLAS order");
+        gatherTrisDevice(meshDescs[i].pos, meshDescs[i].idx, (const int*)order.ptr, nt,
+                         tris + 3 * (size_t)triCursor, st);
+      }
+      cursor += 1;
+    }
+    triCursor += nt;
+  }
+  cudaCheck(cudaStreamSynchronize(st), "device BVH build");
+  numNodes = (size_t)cursor;
+  numTris = (size_t)triCursor;
 }
 
 size_t DeviceScene::table(int which, float* out, size_t cap) const {
@@ -842,6 +980,13 @@ extern "C" int sundog_session_trace_counts(sundog_session* sh, sundog_trace_coun
   SDB_TRY
   if (!sh || !out) throw std::runtime_error("session: null argument");
   reinterpret_cast<RenderSession*>(sh)->countTraversal(out);
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
+
+extern "C" int sundog_set_bvh_builder(int device) {
+  SDB_TRY
+  g_deviceBvh.store(device ? 1 : 0);
   return SUNDOG_OK;
   SDB_CATCH(SUNDOG_ERROR)
 }

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/sundog_api.h"
+#include "assets.h"
 #include "scene_model.h"
 
 namespace sdb {
@@ -56,6 +57,8 @@ struct MeshBufs {
 };
 
 void quadricBoundsHost(int kind, float3& lo, float3& hi);
+// Whether binary BVHs are built on the device (sundog_set_bvh_builder).
+bool deviceBvhBuilds();
 
 struct GuideState;  // guide.h
 struct WfBuffers;   // wavefront.h
@@ -79,6 +82,10 @@ struct DeviceScene {
   std::vector<SdLight> lights;  // host copy of the device light list
 
   void build(const SceneDesc& desc);
+  // The binary BVH of every mesh and the TLAS built on the device into
+  // dNodes / dTris (tlasOrder: TLAS leaf order -> object).
+  void buildAccelOnDevice(const std::vector<HostMesh>& meshes, std::vector<SdMesh>& meshDescs,
+                          std::vector<int>& tlasOrder);
   // Copies sampling table `which` (0 env marginal CDF, 1 env conditional
   // CDFs, 2 + k the area CDF of light k; empty when the scene has none) to
   // out (cap floats); returns its length.
