@@ -291,6 +291,15 @@ SUNDOG_API int sundog_session_trace_counts_split(sundog_session*, sundog_trace_c
  * shade-A, shadow-ray and shade-B stages, the iterations, the radiance and
  * shadow rays traced and the stage launches. Megakernel renders leave it
  * zero. Returns 0/1. */
+/* Denoised copy of the session's film (the replacement of the reference's
+ * OptiX AI denoiser pass, src/denoise.cpp:18-53, with the same albedo and
+ * normal guides): an edge-avoiding a-trous wavelet filter on the GPU. The
+ * session must render AOVs (sundog_render_ext.aov_albedo or aov_normal set
+ * at creation). out: width*height float4, host memory. sundog_render and
+ * sundog_render_ex run the same filter when the scene or the options ask for
+ * denoise, and write / return the denoised film. Returns 0/1. */
+SUNDOG_API int sundog_session_denoise(sundog_session*, float* out);
+
 /* The session's film as sundog's HDR output codes (no counterpart in the
  * reference; src/film.cpp:96-115 computes the same codes on the host before
  * its AVIF encode): x 2^exposure (exposure NaN = the scene's), BT.709 ->

@@ -167,7 +167,7 @@ ADDITIVE_SYMBOLS = [
     "sundog_session_copy_film", "sundog_session_trace_counts_split",
     "sundog_session_set_stage_timing", "sundog_session_stage_times", "sundog_session_table",
     "sundog_set_device_memory_cache", "sundog_release_device_memory", "sundog_session_read_pq12",
-    "sundog_set_bvh_builder",
+    "sundog_set_bvh_builder", "sundog_session_denoise",
 ]
 
 _lib = None
@@ -245,6 +245,7 @@ def load(path=None):
     lib.sundog_session_table.argtypes = [vp, ip, vp, ctypes.c_size_t,
                                          ctypes.POINTER(ctypes.c_size_t)]
     lib.sundog_session_read_pq12.argtypes = [vp, dp, vp]
+    lib.sundog_session_denoise.argtypes = [vp, vp]
     lib.sundog_set_bvh_builder.argtypes = [ip]
     lib.sundog_set_device_memory_cache.argtypes = [ip]
     lib.sundog_release_device_memory.argtypes = []

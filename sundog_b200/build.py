@@ -22,7 +22,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 CU_SOURCES = ["pt_kernel.cu", "selftest.cu", "noalloc.cu", "guide.cu", "serve.cu", "wavefront.cu",
-              "cdf_build.cu", "film_out.cu", "bvh_device.cu"]
+              "cdf_build.cu", "film_out.cu", "bvh_device.cu", "denoise.cu"]
 CPP_SOURCES = ["scene_api.cpp", "scene_derive.cpp", "assets.cpp", "bvh_build.cpp",
                "render.cpp", "render_api.cpp", "serve_host.cpp"]
 

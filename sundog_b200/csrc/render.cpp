@@ -623,8 +623,9 @@ void RenderSession::build(const sundog_scene* h, const sundog_render_options* op
     std::fprintf(stderr,
                  "sundog: physics settling is not part of this renderer; rendering authored "
                  "poses\n");
+  // AOVs when asked for, and as the denoiser's guides when it runs.
   aov = (opt && (opt->aov_albedo_path || opt->aov_normal_path)) ||
-        (ext && (ext->aov_albedo || ext->aov_normal));
+        (ext && (ext->aov_albedo || ext->aov_normal)) || rs.denoise;
   int devId = 0;
   cudaCheck(cudaGetDevice(&devId), "cudaGetDevice");
   cudaCheck(cudaFree(nullptr), "CUDA context");

@@ -20,6 +20,7 @@
 
 #include "../../include/sundog_api.h"
 #include "abi_util.h"
+#include "denoise.h"
 #include "film_out.h"
 #include "guide.h"
 #include "render_session.h"
@@ -108,7 +109,7 @@ std::string jesc(const std::string& s) {
 // Same keys as the reference's stats sidecar (src/stats.cpp:26-61), plus
 // samples_per_sec, the device-timed kernel milliseconds and BVH figures.
 void writeStats(const std::string& path, const char* sceneName, const RenderSession& s,
-                const sundog_render_result& r, double totalMs, size_t peakMB) {
+                const sundog_render_result& r, double totalMs, double denoiseMs, size_t peakMB) {
   FILE* f = std::fopen(path.c_str(), "w");
   if (!f) throw std::runtime_error("cannot write " + path);
   cudaDeviceProp p;
@@ -121,13 +122,13 @@ void writeStats(const std::string& path, const char* sceneName, const RenderSess
   const RenderCfg& rs = s.scene.render;
   std::fprintf(f, "{\n  \"scene\": %s,\n", jesc(sceneName).c_str());
   std::fprintf(f, "  \"width\": %d,\n  \"height\": %d,\n  \"spp\": %d,\n", rs.width, rs.height, rs.spp);
-  std::fprintf(f, "  \"max_depth\": %d,\n  \"seed\": %u,\n  \"denoised\": false,\n", rs.maxDepth,
-               rs.seed);
+  std::fprintf(f, "  \"max_depth\": %d,\n  \"seed\": %u,\n  \"denoised\": %s,\n", rs.maxDepth,
+               rs.seed, rs.denoise ? "true" : "false");
   std::fprintf(f,
                "  \"timings_ms\": {\n    \"scene_load\": %.17g,\n    \"physics\": 0,\n"
-               "    \"gas_build\": %.17g,\n    \"render\": %.17g,\n    \"denoise\": 0,\n"
+               "    \"gas_build\": %.17g,\n    \"render\": %.17g,\n    \"denoise\": %.17g,\n"
                "    \"total\": %.17g\n  },\n",
-               s.loadMs, s.buildMs, r.render_ms, totalMs);
+               s.loadMs, s.buildMs, r.render_ms, denoiseMs, totalMs);
   std::fprintf(f, "  \"rays_traced\": %llu,\n  \"mrays_per_sec\": %.17g,\n",
                (unsigned long long)r.rays_traced, r.mrays_per_sec);
   std::fprintf(f, "  \"samples_per_sec\": %.17g,\n  \"kernel_ms\": %.17g,\n", r.samples_per_sec,
@@ -168,7 +169,7 @@ int renderImpl(sundog_scene* h, const sundog_render_options* opt, const sundog_r
     cudaGetDeviceProperties(&p, dev);
     std::fprintf(stderr, "sundog: %s %dx%d, %d spp, depth %d on %s\n", sceneName, rs.width,
                  rs.height, rs.spp, rs.maxDepth, p.name);
-    if (rs.denoise) std::fprintf(stderr, "sundog: no denoiser in this build; writing the raw film\n");
+
   }
   sundog_render_result r{};
   int reps = ext && ext->repeat > 1 ? ext->repeat : 1;
@@ -183,6 +184,18 @@ int renderImpl(sundog_scene* h, const sundog_render_options* opt, const sundog_r
   }
   r = bestR;
   size_t npix = (size_t)rs.width * rs.height;
+  // Optional post-process (src/capi_render.cpp:247-256): the denoised film
+  // replaces the raw one as the call's output.
+  double denoiseMs = 0.0;
+  DevBuf denoised;
+  if (rs.denoise) {
+    auto tDen = std::chrono::steady_clock::now();
+    denoised.alloc(npix * sizeof(float4));
+    denoiseFilm((const float4*)s->accum.ptr, (const float4*)s->aovAlb.ptr,
+                (const float4*)s->aovNrm.ptr, rs.width, rs.height, denoiseDefaults(),
+                (float4*)denoised.ptr, s->stream);
+    denoiseMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tDen).count();
+  }
   // The film goes straight into the caller's buffer when there is one.
   std::vector<float> own;
   float* film = ext && ext->film_rgba ? ext->film_rgba : nullptr;
@@ -190,7 +203,13 @@ int renderImpl(sundog_scene* h, const sundog_render_options* opt, const sundog_r
     own.resize(npix * 4);
     film = own.data();
   }
-  s->read(film, nullptr, nullptr);
+  if (rs.denoise) {
+    cudaCheck(cudaMemcpy(film, denoised.ptr, npix * sizeof(float4), cudaMemcpyDeviceToHost),
+              "denoised film download");
+    countDownload(npix * sizeof(float4));
+  } else {
+    s->read(film, nullptr, nullptr);
+  }
   std::vector<float> alb, nrm;
   if (s->aov) {
     alb.resize(npix * 4);
@@ -206,8 +225,8 @@ int renderImpl(sundog_scene* h, const sundog_render_options* opt, const sundog_r
     if (avif || endsWith(out, ".png")) {
       if (avif) out = out.substr(0, out.size() - 5) + ".png";
       std::vector<unsigned short> codes(npix * 3);
-      encodePq12((const float4*)s->accum.ptr, rs.width, rs.height, rs.exposure, codes.data(),
-                 s->stream);
+      encodePq12((const float4*)(rs.denoise ? denoised.ptr : s->accum.ptr), rs.width, rs.height,
+                 rs.exposure, codes.data(), s->stream);
       writePq16Png(out, codes.data(), rs.width, rs.height);
       wrote = out;
     } else {
@@ -229,13 +248,29 @@ int renderImpl(sundog_scene* h, const sundog_render_options* opt, const sundog_r
   r.total_ms = totalMs;
   if (opt->stats_path) {
     size_t peak = s->freeBefore > freeAfter ? (s->freeBefore - freeAfter) >> 20 : 0;
-    writeStats(opt->stats_path, sceneName, *s, r, totalMs, peak);
+    writeStats(opt->stats_path, sceneName, *s, r, totalMs, denoiseMs, peak);
   }
   if (res) *res = r;
   return SUNDOG_OK;
 }
 
 }  // namespace
+
+extern "C" int sundog_session_denoise(sundog_session* sh, float* out) {
+  SDB_TRY
+  if (!sh || !out) throw std::runtime_error("denoise: null argument");
+  RenderSession& s = *reinterpret_cast<RenderSession*>(sh);
+  if (!s.aov) throw std::runtime_error("denoise: the session renders no AOVs (create it with AOVs)");
+  size_t npix = (size_t)s.lp.width * s.lp.height;
+  DevBuf d;
+  d.alloc(npix * sizeof(float4));
+  denoiseFilm((const float4*)s.accum.ptr, (const float4*)s.aovAlb.ptr, (const float4*)s.aovNrm.ptr,
+              s.lp.width, s.lp.height, denoiseDefaults(), (float4*)d.ptr, s.stream);
+  cudaCheck(cudaMemcpy(out, d.ptr, npix * sizeof(float4), cudaMemcpyDeviceToHost), "denoise read");
+  countDownload(npix * sizeof(float4));
+  return SUNDOG_OK;
+  SDB_CATCH(SUNDOG_ERROR)
+}
 
 extern "C" int sundog_session_read_pq12(sundog_session* sh, double exposure, uint16_t* out) {
   SDB_TRY

@@ -394,6 +394,15 @@ class Session(object):
                   self.lib)
         return film
 
+    def denoise(self):
+        """The film denoised on the device (needs a session created with
+        aov=True): height x width x 4 float32."""
+        s = self.stats
+        out = np.zeros((s.height, s.width, 4), np.float32)
+        abi.check(self.lib.sundog_session_denoise(self.handle, out.ctypes.data), "denoise",
+                  self.lib)
+        return out
+
     def copy_film(self, film_device_ptr, stream=None):
         """Device-to-device copy of the film into caller-owned device memory
         (width*height float4) on `stream` (a cudaStream_t as int)."""
