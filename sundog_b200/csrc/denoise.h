@@ -6,10 +6,10 @@
 namespace sdb {
 
 struct DenoiseParams {
-  int passes = 5;            // a-trous passes (holes 1, 2, 4, ...)
-  float sigmaColor = 0.4f;   // tone-compressed colour tolerance of the first pass
-  float sigmaNormal = 0.3f;  // normal-AOV tolerance
-  float sigmaAlbedo = 0.1f;  // albedo-AOV tolerance
+  int passes = 4;               // a-trous passes (holes 1, 2, 4, ...)
+  float sigmaLuminance = 4.0f;  // luminance tolerance in local standard deviations
+  float sigmaNormal = 0.2f;     // normal-AOV tolerance
+  float sigmaAlbedo = 0.05f;    // albedo-AOV tolerance
 };
 DenoiseParams denoiseDefaults();
 

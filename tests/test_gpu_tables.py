@@ -86,6 +86,7 @@ def test_black_env_rows_get_uniform_ramps(lib, tmp_path):
     workloads.write_hdr(str(tmp_path / "bands.hdr"), rgb)
     s = sc.Scene()
     s.render(width=8, height=8, spp=1)
+    s.camera(lookfrom=[0, 0, 4], lookat=[0, 0, 0])
     s.background_envmap("bands.hdr")
     s.lambert("grey", color=[0.5, 0.5, 0.5])
     s.add("sphere", "grey")
