@@ -215,7 +215,7 @@ def ncu_traffic_per_path(engine=0):
     (traffic is per-path work: path state between stages, per-sample
     radiance writes, stack lines), so a chunk's traffic is this times its
     paths. engine 1 = the persistent megakernel, else the wavefront engine."""
-    name = "pt_persistent_instancing.md" if engine == 1 else "wf_trace_instancing.md"
+    name = "pt_persistent_instancing.md" if engine == 1 else "wf_render_dram_instancing_small.md"
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.isfile(p):
         return None
