@@ -255,18 +255,19 @@ def profile_figures(name):
 
 def l2_copy_gbps(stream):
     """L2-resident copy bandwidth measured here (read + write bytes over
-    CUDA-event time, best of 20): a 24 MiB float buffer copied into another,
+    CUDA-event time): a 24 MiB float buffer copied into another,
     both held in the 126 MB L2 after the first pass -- the L2 denominator of
-    the trace stage's roofline, measured like the HBM copy peak."""
+    the trace stage's roofline, measured like the HBM copy peak (best of 30
+    after 200 warm-up copies)."""
     import torch
     n = 24 << 18  # 24 MiB of float32
     a = torch.ones(n, dtype=torch.float32, device="cuda")
     b = torch.empty_like(a)
     best = 0.0
     with torch.cuda.stream(stream):
-        for _ in range(3):
+        for _ in range(200):  # clocks up, both buffers resident in L2
             b.copy_(a)
-        for _ in range(20):
+        for _ in range(30):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)

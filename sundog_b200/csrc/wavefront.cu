@@ -23,6 +23,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -149,6 +150,21 @@ __global__ void __launch_bounds__(kRenderBlock) wfStart() {
   for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < pool.cap;
        slot += gridDim.x * blockDim.x)
     refill<GUIDE>(slot, 0);
+}
+
+// Stores a closest-hit candidate straight into the slot's hit record (three
+// 16-byte stores), so the trace loop keeps no hit fields in registers: each
+// closer hit overwrites the record, and a ray that hits nothing leaves the
+// miss marker (inst = -1) written when it was fetched.
+__device__ __forceinline__ void putHit(PoolSlot<TraceHit>& s, float t, int inst, int prim, float u,
+                                       float v, float3 nq, bool front) {
+  static_assert(offsetof(TraceHit, nq) == 20 && offsetof(TraceHit, front) == 32 &&
+                    sizeof(PoolSlot<TraceHit>) == 48,
+                "TraceHit layout assumed by the vector stores");
+  float4* p = reinterpret_cast<float4*>(&s);
+  p[0] = make_float4(t, __int_as_float(inst), __int_as_float(prim), u);
+  p[1] = make_float4(v, nq.x, nq.y, nq.z);
+  p[2] = make_float4(__int_as_float(front ? 1 : 0), 0.0f, 0.0f, 0.0f);
 }
 
 // Idle lanes a warp gathers before it fetches new rays (measured on the
@@ -346,11 +362,12 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
   unsigned long long rays = 0;
   int slot = -1;
   bool exhausted = false;  // warp-uniform
-  float3 O = v3(0.0f), D = v3(0.0f), ro = v3(0.0f), rd = v3(0.0f), id = v3(0.0f), oi = v3(0.0f);
+  // The current space's ray (world in the TLAS, object space in a BLAS); the
+  // world ray is re-read from the slot when a BLAS is left.
+  float3 ro = v3(0.0f), rd = v3(0.0f), id = v3(0.0f), oi = v3(0.0f);
   WtRay wr;
-  float tmax = 0.0f;
-  TraceHit hit;
-  bool found = false, inBlas = false;
+  float tmax = 0.0f;  // the closest accepted hit so far (1e16: none)
+  bool inBlas = false;
   int curInst = -1, cur = kPop, sp = 0;
   int stack[kStackSize];
   while (true) {
@@ -367,14 +384,12 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
           slot = pool.lists[in][i];
           if (SERVE) job = pool.jobs[slot];
           const SdLaunch& jl = SERVE ? c_wjobs[job] : c_wlp;
-          O = pool.paths[slot].v.o;
-          D = pool.paths[slot].v.d;
-          ro = O;
-          rd = D;
+          ro = pool.paths[slot].v.o;
+          rd = pool.paths[slot].v.d;
           id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
           oi = ro * id;
           tmax = 1e16f;
-          found = false;
+          pool.hits[slot].v.inst = -1;  // a miss until a hit is stored
           inBlas = false;
           curInst = -1;
           sp = 0;
@@ -411,9 +426,7 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
       continue;
     }
     if (cur == kPop) {
-      if (sp == 0) {  // ray done
-        if (!found) hit.inst = -1;
-        pool.hits[slot].v = hit;
+      if (sp == 0) {  // ray done: its closest hit is already in the slot
         rays++;
         slot = -1;
         continue;
@@ -421,8 +434,8 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
       cur = stack[--sp];
       if (cur == kToTlas) {
         inBlas = false;
-        ro = O;
-        rd = D;
+        ro = pool.paths[slot].v.o;
+        rd = pool.paths[slot].v.d;
         id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
         oi = ro * id;
         cur = kPop;
@@ -437,7 +450,7 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
     if (!inBlas) {
       // TLAS leaves hold exactly one instance.
       const SdInstance& inst = lp.inst[start];
-      float3 o2 = xfPoint(inst.w2o, O), d2 = xfVec(inst.w2o, D);
+      float3 o2 = xfPoint(inst.w2o, ro), d2 = xfVec(inst.w2o, rd);  // ro, rd: world here
       if (inst.kind == GK_MESH) {
         if (sp < kStackSize) {
           stack[sp++] = kToTlas;
@@ -459,14 +472,7 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
         bool front = dot(q.n, d2) < 0.0f;
         if ((inst.flags & kInstMasked) && !faceAccepts(lp, inst, front, q.u, q.v)) continue;
         tmax = q.t;
-        found = true;
-        hit.t = q.t;
-        hit.inst = start;
-        hit.prim = 0;
-        hit.u = q.u;
-        hit.v = q.v;
-        hit.nq = q.n;
-        hit.front = front;
+        putHit(pool.hits[slot], q.t, start, 0, q.u, q.v, q.n, front);
       }
       continue;
     }
@@ -484,18 +490,12 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
       if (!needFace) {
         front = dot(cross(p1 - p0, p2 - p0), rd) < 0.0f;
       } else {
-        ShadePt spt = triShade(lp, inst, prim, b1, b2, D);
+        ShadePt spt = triShade(lp, inst, prim, b1, b2, pool.paths[slot].v.d);
         if ((inst.flags & kInstMasked) && !faceAccepts(lp, inst, spt.front, spt.u, spt.v)) continue;
         front = spt.front;
       }
       tmax = t;
-      found = true;
-      hit.t = t;
-      hit.inst = curInst;
-      hit.prim = prim;
-      hit.u = b1;
-      hit.v = b2;
-      hit.front = front;
+      putHit(pool.hits[slot], t, curInst, prim, b1, b2, v3(0.0f), front);
     }
   }
   addRays<SERVE ? kWfServe : 0>(rays);
