@@ -506,6 +506,16 @@ typedef struct {
 SUNDOG_API void sundog_server_defaults(sundog_server_config* config);
 /* config NULL = defaults. Returns NULL on error (sundog_last_error). */
 SUNDOG_API sundog_server* sundog_server_create(const sundog_server_config* config);
+/* The same on a given device (0 .. sundog_device_count() - 1): the server's
+ * thread, stream, pool and scene cache live there. One server per device is
+ * how several GPUs serve together (sundog_b200/serve.py MultiServer places
+ * each job on the device with the least queued work); servers and sessions
+ * may share a device (a per-device lock orders their launches). Returns NULL
+ * on failure. */
+SUNDOG_API sundog_server* sundog_server_create_on_device(const sundog_server_config*,
+                                                        int device);
+/* CUDA devices visible to the library, or -1 when the runtime cannot tell. */
+SUNDOG_API int sundog_device_count(void);
 /* Queues a render of the scene (copied: the handle may be destroyed after the
  * call). options: width / height / spp / seed / transparent_shadows / clamp
  * overrides as in sundog_render (NULL = the scene's). film_rgba: host buffer

@@ -167,7 +167,8 @@ ADDITIVE_SYMBOLS = [
     "sundog_session_copy_film", "sundog_session_trace_counts_split",
     "sundog_session_set_stage_timing", "sundog_session_stage_times", "sundog_session_table",
     "sundog_set_device_memory_cache", "sundog_release_device_memory", "sundog_session_read_pq12",
-    "sundog_set_bvh_builder", "sundog_session_denoise",
+    "sundog_set_bvh_builder", "sundog_session_denoise", "sundog_server_create_on_device",
+    "sundog_device_count",
 ]
 
 _lib = None
@@ -271,6 +272,9 @@ def load(path=None):
     lib.sundog_server_defaults.restype = None
     lib.sundog_server_create.argtypes = [ctypes.POINTER(ServerConfig)]
     lib.sundog_server_create.restype = vp
+    lib.sundog_server_create_on_device.argtypes = [ctypes.POINTER(ServerConfig), ip]
+    lib.sundog_server_create_on_device.restype = vp
+    lib.sundog_device_count.argtypes = []
     lib.sundog_server_submit.argtypes = [vp, vp, ctypes.POINTER(RenderOptions), vp]
     lib.sundog_server_submit.restype = ctypes.c_int64
     lib.sundog_server_status.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(JobStatus)]

@@ -406,6 +406,19 @@ void DeviceScene::build(const SceneDesc& desc) {
   deviceBytes = freeBefore > freeB ? freeBefore - freeB : 0;
 }
 
+// One lock per device over the launch blocks kept in constant memory (the
+// render and server kernels read their scene, film and job tables from
+// there): whoever writes them holds the lock until the kernels that read
+// them have finished, so sessions and servers in different host threads can
+// share a device.
+static std::mutex g_launchLocks[64];
+std::mutex& deviceLaunchLock() {
+  int dev = 0;
+  cudaCheck(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
+  return g_launchLocks[dev];
+}
+
 // Which builder makes the binary BVH (sundog_set_bvh_builder): 1 = on the
 // device (default), 0 = the host binned-SAH builder.
 static std::atomic<int> g_deviceBvh{1};
@@ -765,25 +778,32 @@ void RenderSession::render(cudaStream_t st, bool reset, sundog_render_result* re
     lp.sppThisLaunch = n;
     lp.numPaths = (unsigned long long)pathsPerSample(lp) * n;
     cudaCheck(cudaMemsetAsync(lp.pathCounter, 0, sizeof(unsigned long long), st), "counter reset");
-    cudaCheck(setLaunch(lp, st), "launch params");
-    cudaCheck(cudaEventRecord(kev[0], st), "event");
-    const bool wavefront = engine != 1;
-    if (lp.numPaths == 0) {
-      // A tile shard that owns no tile: nothing to trace.
-    } else if (wavefront) {
-      if (!wf) wf = wfAcquire();
-      wf->ensure((int)std::min<unsigned long long>(lp.numPaths, kWavefrontSlots));
-      launches += wfRender(lp, *wf, st, mode, stageTiming ? &stages : nullptr);
-    } else {
-      cudaCheck(launchRender(st, grid, mode), "path kernel launch");
-      launches += 1;
+    {
+      // The launch blocks live in per-device constant memory: hold the
+      // device's launch lock from writing them until the chunk's last kernel
+      // that reads them (the fold) has finished.
+      std::lock_guard<std::mutex> launchLock(deviceLaunchLock());
+      cudaCheck(setLaunch(lp, st), "launch params");
+      cudaCheck(cudaEventRecord(kev[0], st), "event");
+      const bool wavefront = engine != 1;
+      if (lp.numPaths == 0) {
+        // A tile shard that owns no tile: nothing to trace.
+      } else if (wavefront) {
+        if (!wf) wf = wfAcquire();
+        wf->ensure((int)std::min<unsigned long long>(lp.numPaths, kWavefrontSlots));
+        launches += wfRender(lp, *wf, st, mode, stageTiming ? &stages : nullptr);
+      } else {
+        cudaCheck(launchRender(st, grid, mode), "path kernel launch");
+        launches += 1;
+      }
+      cudaCheck(cudaEventRecord(kev[1], st), "event");
+      cudaCheck(cudaEventSynchronize(kev[1]), "path kernel");
+      float one = 0.0f;
+      cudaCheck(cudaEventElapsedTime(&one, kev[0], kev[1]), "event time");
+      kms += one;
+      cudaCheck(launchFold((int)npix, st), "fold launch");
+      cudaCheck(cudaStreamSynchronize(st), "fold");
     }
-    cudaCheck(cudaEventRecord(kev[1], st), "event");
-    cudaCheck(cudaEventSynchronize(kev[1]), "path kernel");
-    float one = 0.0f;
-    cudaCheck(cudaEventElapsedTime(&one, kev[0], kev[1]), "event time");
-    kms += one;
-    cudaCheck(launchFold((int)npix, st), "fold launch");
     launches += 1;
     done += n;
     if (mode & kGuideRecord) {
@@ -828,9 +848,11 @@ void RenderSession::countTraversal(sundog_trace_counts* out, sundog_trace_counts
     lp.sppThisLaunch = n;
     lp.numPaths = (unsigned long long)pathsPerSample(lp) * n;
     cudaCheck(cudaMemsetAsync(lp.pathCounter, 0, sizeof(unsigned long long), stream), "counter reset");
+    std::lock_guard<std::mutex> launchLock(deviceLaunchLock());
     cudaCheck(setLaunch(lp, stream), "launch params");
     cudaCheck(launchRenderCounting(stream, grid, (TraceCount*)dc.ptr), "counting launch");
     cudaCheck(launchFold((int)npix, stream), "fold launch");
+    cudaCheck(cudaStreamSynchronize(stream), "counting chunk");
     done += n;
   }
   cudaCheck(cudaStreamSynchronize(stream), "counting render");

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -59,6 +60,9 @@ struct MeshBufs {
 void quadricBoundsHost(int kind, float3& lo, float3& hi);
 // Whether binary BVHs are built on the device (sundog_set_bvh_builder).
 bool deviceBvhBuilds();
+// The current device's launch lock (render.cpp): held from writing the
+// constant-memory launch blocks until the kernels reading them are done.
+std::mutex& deviceLaunchLock();
 
 struct GuideState;  // guide.h
 struct WfBuffers;   // wavefront.h

@@ -112,9 +112,8 @@ __global__ void ptServeFold() {
   }
 }
 
-cudaError_t serveSetJob(int slot, const SdLaunch& lp, cudaStream_t st) {
-  if (slot < 0 || slot >= kMaxServeJobs) return cudaErrorInvalidValue;
-  return cudaMemcpyToSymbolAsync(c_jobs, &lp, sizeof(SdLaunch), slot * sizeof(SdLaunch),
+cudaError_t serveSetJobs(const SdLaunch* table, cudaStream_t st) {
+  return cudaMemcpyToSymbolAsync(c_jobs, table, kMaxServeJobs * sizeof(SdLaunch), 0,
                                  cudaMemcpyHostToDevice, st);
 }
 

@@ -32,7 +32,9 @@ struct ServeBatch {
 
 // Writes a job's launch block into slot `slot` of the device job table
 // (ordered on st before later launches).
-cudaError_t serveSetJob(int slot, const SdLaunch& lp, cudaStream_t st);
+// The whole job table (kMaxServeJobs launch blocks, host memory; unused slots
+// zero) into the megakernel server's constant memory.
+cudaError_t serveSetJobs(const SdLaunch* table, cudaStream_t st);
 int serveGridSize();
 // The batch's persistent render launch followed by its fold launch.
 cudaError_t serveLaunch(const ServeBatch& batch, int grid, cudaStream_t st);

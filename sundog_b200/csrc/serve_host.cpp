@@ -353,9 +353,7 @@ class Server {
     j->lp.accum = (float4*)j->film.ptr;
     j->lp.sampleOffset = 0;
     j->lp.sppThisLaunch = j->spp;
-    cudaCheck(serveSetJob(slot, j->lp, st), "job table");
-    if (wf) cudaCheck(wfSetJob(slot, j->lp, st), "job table");
-    j->slot = slot;
+    j->slot = slot;  // its launch block is uploaded with every batch
     slots[slot] = j;
     j->tilesX = (j->width + cfg.tile - 1) / cfg.tile;
     j->tilesY = (j->height + cfg.tile - 1) / cfg.tile;
@@ -472,6 +470,15 @@ class Server {
       while (total + itemMax <= cfg.iteration_paths && add(i)) {
       }
     if (n == 0) return;
+    // The job table and batch block live in per-device constant memory,
+    // shared with sessions and other servers on the device: upload them and
+    // run the batch to completion under the device's launch lock.
+    std::lock_guard<std::mutex> launchLock(deviceLaunchLock());
+    std::vector<SdLaunch> table(kMaxServeJobs);
+    std::memset(table.data(), 0, table.size() * sizeof(SdLaunch));
+    for (size_t k = 0; k < slots.size(); k++)
+      if (slots[k]) table[k] = slots[k]->lp;
+    cudaCheck(wf ? wfSetJobs(table.data(), st) : serveSetJobs(table.data(), st), "job table");
     cudaCheck(cudaMemcpyAsync(dItems.ptr, hItems, (size_t)n * sizeof(ServeItem),
                               cudaMemcpyHostToDevice, st),
               "batch items");
@@ -623,6 +630,26 @@ extern "C" sundog_server* sundog_server_create(const sundog_server_config* c) {
     throw std::runtime_error("server: iteration_paths is smaller than one tile-pass");
   return reinterpret_cast<sundog_server*>(new Server(cfg));
   SDB_CATCH(nullptr)
+}
+
+extern "C" sundog_server* sundog_server_create_on_device(const sundog_server_config* c,
+                                                        int device) {
+  SDB_TRY
+  int count = 0;
+  cudaCheck(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+  if (device < 0 || device >= count) throw std::runtime_error("server: no such device");
+  int prev = 0;
+  cudaCheck(cudaGetDevice(&prev), "cudaGetDevice");
+  cudaCheck(cudaSetDevice(device), "cudaSetDevice");
+  sundog_server* sv = sundog_server_create(c);  // the server keeps the device current then
+  cudaSetDevice(prev);
+  return sv;
+  SDB_CATCH(nullptr)
+}
+
+extern "C" int sundog_device_count(void) {
+  int n = 0;
+  return cudaGetDeviceCount(&n) == cudaSuccess ? n : -1;
 }
 
 extern "C" int64_t sundog_server_submit(sundog_server* sv, sundog_scene* h,

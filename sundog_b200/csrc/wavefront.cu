@@ -770,9 +770,8 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide, WfSta
   return runPool(b, st, lp.numPaths, guide, times);
 }
 
-cudaError_t wfSetJob(int slot, const SdLaunch& lp, cudaStream_t st) {
-  if (slot < 0 || slot >= kMaxServeJobs) return cudaErrorInvalidValue;
-  return cudaMemcpyToSymbolAsync(c_wjobs, &lp, sizeof(SdLaunch), slot * sizeof(SdLaunch),
+cudaError_t wfSetJobs(const SdLaunch* table, cudaStream_t st) {
+  return cudaMemcpyToSymbolAsync(c_wjobs, table, kMaxServeJobs * sizeof(SdLaunch), 0,
                                  cudaMemcpyHostToDevice, st);
 }
 

@@ -79,11 +79,12 @@ bool keepDeviceMemory();
 int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide = 0,
              WfStageTimes* times = nullptr);
 
-// Serving batches (serve.h): job slot `slot` of the engine's job table, and
-// one batch of tile-passes rendered through the pool into batch.sampleL at
-// each path's id (the caller folds them). Returns the kernels launched.
+// Serving batches (serve.h): the engine's whole job table (kMaxServeJobs
+// launch blocks, host memory), and one batch of tile-passes rendered through
+// the pool into batch.sampleL at each path's id (the caller folds them).
+// Returns the kernels launched.
 struct ServeBatch;
-cudaError_t wfSetJob(int slot, const SdLaunch& lp, cudaStream_t st);
+cudaError_t wfSetJobs(const SdLaunch* table, cudaStream_t st);
 int wfRenderBatch(const ServeBatch& batch, WfBuffers& b, cudaStream_t st);
 
 }  // namespace sdb

@@ -134,3 +134,50 @@ def test_single_slot_serialises_jobs(lib):
         assert b.last.queued_ms >= a.last.latency_ms - 50.0
         assert b.last.latency_ms > a.last.latency_ms
         assert sv.stats().scenes_resident == 1
+
+
+def test_servers_and_sessions_share_a_device(lib, asset_dir):
+    """Two servers on one device (what MultiServer does across devices, here
+    on the one GPU a test gets) and a session rendering from this thread at
+    the same time: each film is the one its job gets alone. The launch
+    blocks all three use live in the device's constant memory; the
+    per-device launch lock orders their batches and chunks."""
+    import threading
+    jobs = mix(asset_dir)
+    cfg = dict(tile=32, pass_spp=4, iteration_paths=1 << 16, engine=0)
+    alone = []
+    for s, o in jobs:
+        with serve.Server(**cfg) as sv:
+            alone.append(sv.submit(s, base_dir=asset_dir, **o).wait())
+    sref = session_film(workloads.cornell(), ".", engine=0, width=160, height=120, spp=16)
+    ms = serve.MultiServer(devices=[0, 0], **cfg)
+    try:
+        handles = [ms.submit(s, base_dir=asset_dir, **o) for s, o in jobs]
+        assert sorted(set(h.placement for h in handles)) == [0, 1]
+        out = {}
+
+        def session_renders():
+            out["films"] = [session_film(workloads.cornell(), ".", engine=0, width=160,
+                                         height=120, spp=16) for _ in range(3)]
+        t = threading.Thread(target=session_renders)
+        t.start()
+        films = [h.wait() for h in handles]
+        t.join()
+    finally:
+        ms.close()
+    for f, a in zip(films, alone):
+        assert np.array_equal(f, a)
+    for f in out["films"]:
+        assert np.array_equal(f, sref)
+
+
+def test_multi_server_on_every_device(lib):
+    """MultiServer over all visible devices (one here): jobs complete and
+    equal the plain server's films."""
+    s = workloads.cornell()
+    with serve.Server() as sv:
+        ref = sv.submit(s, width=64, height=64, spp=4).wait()
+    with serve.MultiServer() as ms:
+        assert len(ms.servers) == lib.sundog_device_count() >= 1
+        film = ms.submit(s, width=64, height=64, spp=4).wait()
+    assert np.array_equal(film, ref)

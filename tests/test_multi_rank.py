@@ -102,3 +102,52 @@ def test_owner_map_tiles():
     assert shard.owned_pixels(200, 130, 16, 13) == 0
     films = [np.where((own == r)[..., None], float(r + 1), 0.0) for r in range(5)]
     assert np.array_equal(shard.assemble(films)[..., 0], own + 1.0)
+
+
+def test_multi_server_places_jobs_on_least_loaded_device():
+    """MultiServer's placement, with stand-in servers (no GPU): each job goes
+    to the server with the fewest queued camera paths; finished jobs stop
+    counting."""
+    from sundog_b200 import abi, serve, workloads
+
+    class FakeJob(object):
+        def __init__(self, jid):
+            self.id = jid
+            self.state = abi.JOB_QUEUED
+
+        def status(self):
+            class S(object):
+                pass
+            st = S()
+            st.state = self.state
+            return st
+
+    class FakeServer(object):
+        def __init__(self):
+            self.jobs = []
+
+        def submit(self, scene, base_dir=".", film=True, **opts):
+            j = FakeJob(len(self.jobs))
+            self.jobs.append(j)
+            return j
+
+        def stats(self):
+            return len(self.jobs)
+
+        def close(self):
+            pass
+
+    assert serve.least_loaded([5, 3, 3, 9]) == 1
+    fakes = [FakeServer(), FakeServer(), FakeServer()]
+    ms = serve.MultiServer(servers=fakes)
+    s = workloads.cornell()
+    big = ms.submit(s, width=1024, height=1024, spp=64)    # -> 0
+    a = ms.submit(s, width=256, height=256, spp=16)        # -> 1
+    b = ms.submit(s, width=256, height=256, spp=16)        # -> 2
+    c = ms.submit(s, width=256, height=256, spp=16)        # -> 1 (tie with 2: first)
+    assert [big.placement, a.placement, b.placement, c.placement] == [0, 1, 2, 1]
+    assert ms.load(0) == 1024 * 1024 * 64
+    big.state = abi.JOB_DONE                               # finished: no longer counts
+    d = ms.submit(s, width=512, height=512, spp=16)
+    assert d.placement == 0 and ms.load(0) == 512 * 512 * 16
+    assert ms.stats() == [2, 2, 1]
