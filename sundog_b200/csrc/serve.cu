@@ -96,6 +96,7 @@ __global__ void ptServeFold() {
   const ServeBatch& b = c_batch;
   const ServeItem& it = b.items[blockIdx.x];
   const SdLaunch& lp = c_jobs[it.job];
+  if (!lp.accum) return;  // an empty table slot: nothing to fold into
   const int npt = it.w * it.h;
   for (int q = threadIdx.x; q < npt; q += blockDim.x) {
     int lx = q % it.w, ly = q / it.w;

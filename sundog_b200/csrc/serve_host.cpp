@@ -478,7 +478,10 @@ class Server {
     std::memset(table.data(), 0, table.size() * sizeof(SdLaunch));
     for (size_t k = 0; k < slots.size(); k++)
       if (slots[k]) table[k] = slots[k]->lp;
-    cudaCheck(wf ? wfSetJobs(table.data(), st) : serveSetJobs(table.data(), st), "job table");
+    // Both engines fold through ptServeFold, which reads the megakernel's
+    // table; the wavefront stages read their own.
+    cudaCheck(serveSetJobs(table.data(), st), "job table");
+    if (wf) cudaCheck(wfSetJobs(table.data(), st), "job table");
     cudaCheck(cudaMemcpyAsync(dItems.ptr, hItems, (size_t)n * sizeof(ServeItem),
                               cudaMemcpyHostToDevice, st),
               "batch items");
