@@ -16,7 +16,7 @@
 // learned guide and/or record training samples; GUIDE = 0 is the plain
 // reference sampler with no guiding code compiled in.
 //
-// The bounce body restates device/programs.cu:311-572 (cited inline).
+// The path segment (bounce, pt_path.cuh) follows device/programs.cu:311-572.
 #include "pt_path.cuh"
 
 namespace sdb {

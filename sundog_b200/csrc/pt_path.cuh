@@ -326,163 +326,27 @@ __device__ __forceinline__ bool finishVertex(const SdLaunch& lp, Path& p, const 
   return p.depth < lp.maxDepth;
 }
 
-// One segment of the path in one piece, for the persistent kernels: trace,
-// media, surface or escape, NEE, BSDF sample, roulette. Returns false when
-// the path has ended. GUIDE selects the guided variants (kGuideSample: draw by
-// MIS with the guide; kGuideRecord: keep training vertices in *trail); 0 is
-// the reference's sampler. It is shadeVertex, the shadow ray and finishVertex
-// written as one function: the same operations in the same order (the
-// engines' equality test holds them together); one body keeps the
-// megakernel's register allocation 6% faster than calling the halves.
-// (device/programs.cu:374-558)
+// One segment of the path for the persistent kernels: the radiance ray,
+// shadeVertex, the shadow ray and finishVertex -- the same functions the
+// wavefront stages call, in the same order with the same random draws, so
+// both engines trace the same samples. Returns false when the path has
+// ended. GUIDE selects the guided variants (kGuideSample: draw by MIS with
+// the guide; kGuideRecord: keep training vertices in *trail); 0 is the
+// reference's sampler. (device/programs.cu:374-558)
 template <bool COUNT, int GUIDE = 0>
 __device__ __forceinline__ bool bounce(const SdLaunch& lp, Path& p, unsigned long long& rays,
                                        TraceCount* cnt, GuideTrail* trail = nullptr) {
-  const bool hasEnv = lp.bgKind == BG_ENVMAP;
-  const int nStrat = lp.numLights + (hasEnv ? 1 : 0);
-
   TraceHit h;
   float dummyTr = 1.0f;
   float3 dummyTau = v3(0.0f);
-  bool hit = traverse<false, COUNT>(lp, p.o, p.d, 1e16f, h, dummyTr, dummyTau, cnt);
+  const bool hit = traverse<false, COUNT>(lp, p.o, p.d, 1e16f, h, dummyTr, dummyTau, cnt);
   rays++;
-
-  if (p.medDepth > 0) {
-    int top = min(p.medDepth, 4) - 1;
-    float3 sigma = lp.materials[medAt(p.med, top)].absorb;
-    if (hmax(sigma) > 0.0f) p.beta *= vexp(-sigma * (hit ? h.t : 1e4f));
-  }
-
-  if (lp.numFlames > 0) {
-    float3 trans = v3(1.0f);
-    float3 Lv = flameMarch(lp.flames, lp.numFlames, p.o, p.d, hit ? h.t : 1e16f, p.rng, trans);
-    addClamped(lp, p, p.beta * Lv);
-    p.beta *= trans;
-  }
-
-  if (!hit) {
-    float3 bg = background(lp, p.d);
-    float w = 1.0f;
-    if (hasEnv && !p.specular) {
-      float pdfE = envDensity(lp.env, p.d) / nStrat;
-      w = p.prevPdf / (p.prevPdf + pdfE);
-    }
-    addClamped(lp, p, p.beta * bg * w);
-    if (p.depth == 0) writeAov(lp, p, v3(fminf(bg.x, 1.0f), fminf(bg.y, 1.0f), fminf(bg.z, 1.0f)), v3(0.0f));
-    return false;
-  }
-
-  const SdInstance& in = lp.inst[h.inst];
-  ShadePt sp = in.kind == GK_MESH ? triShade(lp, in, h.prim, h.u, h.v, p.d)
-                                  : quadShade(in, h.nq, h.u, h.v, p.d);
-  bool front = h.front;
-  int matId = front ? (int)(in.mats & 0xFFFF) : (int)(in.mats >> 16);
-  float3 ns = front ? sp.nFront : -sp.nFront;
-  float3 x = p.o + h.t * p.d;
-  const SdMaterial mat = lp.materials[matId];
-  float3 albedo = surfaceAlbedo(mat, lp.textures, sp.u, sp.v);
-  if (mat.kind == MT_WATER && mat.waveAmp > 0.0f)
-    ns = waveNormal(x, ns, -p.d, mat.waveAmp, mat.waveFreq);
-
-  if (p.depth == 0) {
-    const SdCamera& cam = lp.cam;
-    writeAov(lp, p, albedo, v3(dot(ns, cam.u), dot(ns, cam.v), dot(ns, cam.w)));
-  }
-
-  if (mat.kind == MT_EMISSIVE) {
-    if (front || mat.twoSided) {
-      float3 Le = albedo * mat.intensity;
-      float w = 1.0f;
-      if (!p.specular && in.lightId >= 0 && lp.numLights > 0) {
-        float pdfL = lightDensity(lp.lights[in.lightId], p.prevX, x, ns) / nStrat;
-        w = p.prevPdf / (p.prevPdf + pdfL);
-      }
-      addClamped(lp, p, p.beta * Le * w);
-    }
-    return false;
-  }
-
-  // Relative index at this interface from the medium stack.
-  float etaExt = 1.0f;
-  if (mat.kind == MT_DIELECTRIC || mat.kind == MT_WATER) {
-    int outer = min(front ? p.medDepth : p.medDepth - 1, 4);
-    if (outer > 0) etaExt = lp.materials[medAt(p.med, outer - 1)].ior;
-  }
-  float etaRel = front ? etaExt / mat.ior : mat.ior / etaExt;
-
-  // Next-event estimation with the balance heuristic.
-  if (nStrat > 0 && !isDeltaMaterial(mat)) {
-    int k = min((int)(p.rng.uni() * nStrat), nStrat - 1);
-    LightDraw ls = k < lp.numLights ? lightDraw(lp.lights[k], x, p.rng, lp.textures)
-                                    : envDraw(lp.env, p.rng);
-    float cosS = ls.ok ? dot(ls.wi, ns) : 0.0f;
-    bool transmitNee = cosS < 0.0f && mat.kind == MT_DIELECTRIC;
-    if (ls.ok && (cosS > 0.0f || transmitNee)) {
-      rays++;
-      float3 so = nudge(x, transmitNee ? -ns : ns);
-      float tmaxS = ls.dist * 0.999f;
-      // Counting build: shadow traversals go to the second counter set.
-      float3 tr = shadowTransmittance<COUNT>(lp, so, ls.wi, tmaxS, COUNT ? cnt + 1 : nullptr);
-      if (hmax(tr) > 0.0f) {
-        if (lp.numFlames > 0 && lp.transparentShadows) {
-          int skip = k < lp.numLights ? lp.lights[k].flameId : -1;
-          tr = tr * flameShadow(lp.flames, lp.numFlames, so, ls.wi, tmaxS, p.rng, skip);
-        }
-        float pdfLe = (ls.delta ? 1.0f : ls.pdf) / nStrat;
-        float3 f = bsdfValue(mat, albedo, -p.d, ls.wi, ns, etaRel);
-        float w = 1.0f;
-        if (!ls.delta) {
-          float pdfB = bsdfDensity(mat, -p.d, ls.wi, ns, etaRel);
-          w = pdfLe / (pdfLe + pdfB);
-        }
-        float3 c = p.beta * f * fabsf(cosS) * ls.Li * w / pdfLe;
-        c = c * tr;
-        if (p.depth >= 1 && lp.clampVal > 0.0f) c = vmin(c, v3(lp.clampVal));
-        p.L += sanitize3(c);
-      }
-    }
-  }
-
-  BsdfDraw bs;
-  float pdfSample;  // density wi was drawn with (differs from bs.pdf when guided)
-  if ((GUIDE & kGuideSample) && guideEligible(mat)) {
-    GuidedDraw gd = guidedDraw(lp, mat, albedo, p.d, ns, front, etaExt, etaRel, x, p.rng);
-    bs = gd.s;
-    pdfSample = gd.pdfSample;
-  } else {
-    bs = bsdfDraw(mat, albedo, p.d, ns, front, etaExt, p.rng);
-    pdfSample = bs.pdf;
-  }
-  if (!bs.ok) return false;
-  if ((mat.kind == MT_WATER || mat.kind == MT_DIELECTRIC) && dot(bs.wi, ns) < 0.0f) {
-    if (front) {
-      if (p.medDepth < 4) {
-        unsigned long long sh = 16ull * p.medDepth;
-        p.med = (p.med & ~(0xFFFFull << sh)) | ((unsigned long long)matId << sh);
-      }
-      p.medDepth++;
-    } else if (p.medDepth > 0) {
-      p.medDepth--;
-    }
-  }
-  if ((GUIDE & kGuideRecord) && !bs.delta && guideEligible(mat))
-    guideRecord(*trail, x, ns, bs.wi, pdfSample, p.beta * bs.weight, p.L);
-  p.beta *= bs.weight;
-  p.specular = bs.delta;
-  p.prevPdf = bs.delta ? 0.0f : bs.pdf;
-  p.prevX = x;
-  float3 offN = dot(bs.wi, ns) >= 0.0f ? ns : -ns;
-  p.o = nudge(x, offN);
-  p.d = bs.wi;
-
-  if (p.depth >= 4) {
-    float q = clampf(hmax(p.beta), 0.05f, 0.95f);
-    if (p.rng.uni() >= q) return false;
-    p.beta *= 1.0f / q;
-  }
-  if (hmax(p.beta) <= 0.0f) return false;
-  p.depth++;
-  return p.depth < lp.maxDepth;
+  Vertex v;
+  if (!shadeVertex<COUNT>(lp, p, hit, h, rays, v)) return false;
+  float3 tr = v3(0.0f);
+  // Counting build: shadow traversals go to the second counter set.
+  if (v.nee) tr = shadowTransmittance<COUNT>(lp, v.so, v.wi, v.tmaxS, COUNT ? cnt + 1 : nullptr);
+  return finishVertex<GUIDE>(lp, p, v, tr, trail);
 }
 
 }  // namespace sdb

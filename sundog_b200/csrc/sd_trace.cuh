@@ -506,161 +506,220 @@ __device__ SDB_TRAVERSE_INLINE bool traverse(const SdLaunch& lp, float3 O, float
 }
 
 #else
+// One ray's walk over the binary two-level BVH, advanced one action at a
+// time by binTravStep: a node visit (both child boxes) or a leaf (a TLAS
+// instance: quadric roots or entry into its BLAS; or a BLAS leaf's
+// triangles), each followed by a pop when nothing is left to descend into.
+// traverse() runs it to the end for one ray; the wavefront trace stage
+// (wavefront.cu) interleaves many rays' walks per warp with dynamic ray
+// fetch. Both visit the same nodes in the same order.
+//
+// The walk's scalars; its stack is a separate per-thread array (an aggregate
+// holding an indexed array would be placed whole in local memory, scalars
+// included).
+struct BinTrav {
+  float3 ro, rd, id, oi;  // the current space's ray: world in the TLAS, object in a BLAS
+  WtRay wr;               // watertight-test constants of rd (inside a BLAS)
+  float tmax;             // closest accepted hit so far (radiance) / the segment's end
+  int cur, sp, curInst;
+  bool inBlas;
+};
+typedef int TravStack[kStackSize];
+
+__device__ __forceinline__ void binTravStart(BinTrav& t, const SdLaunch& lp, float3 o, float3 d,
+                                             float tmax) {
+  t.ro = o;
+  t.rd = d;
+  t.id = v3(safeInv(d.x), safeInv(d.y), safeInv(d.z));
+  t.oi = o * t.id;
+  t.tmax = tmax;
+  t.sp = 0;
+  t.inBlas = false;
+  t.curInst = -1;
+  t.cur = lp.numInstances > 0 ? lp.tlasRoot : kPop;
+}
+
+// Outcome of one step.
+constexpr int kTravDone = 0;      // every node visited
+constexpr int kTravMore = 1;      // more steps to take
+constexpr int kTravOccluded = 2;  // shadow rays: an opaque crossing
+
+// Takes the next stack entry into t.cur, the step that ends a node or a leaf
+// with nothing left to descend into (done in that same step, so no loop
+// iteration is spent on a pop alone). A BLAS marker restores the world ray
+// and the entry below it is taken (a TLAS entry: BLASes do not nest).
+// Returns kTravDone when the stack is empty.
+template <class Sink>
+__device__ __forceinline__ int binTravPop(BinTrav& t, TravStack& stack, Sink& sink) {
+  if (t.sp == 0) return kTravDone;
+  int c = stack[--t.sp];
+  if (c == kToTlas) {
+    t.inBlas = false;
+    sink.world(t.ro, t.rd);
+    t.id = v3(safeInv(t.rd.x), safeInv(t.rd.y), safeInv(t.rd.z));
+    t.oi = t.ro * t.id;
+    if (t.sp == 0) return kTravDone;
+    c = stack[--t.sp];
+  }
+  t.cur = c;
+  return kTravMore;
+}
+
+// One action of the walk. The sink receives what the walk finds and owns
+// the world ray: sink.world(ro, rd) restores it when the walk leaves a BLAS,
+// sink.worldDir() is the world direction for shading a candidate, and
+// (radiance rays) sink.hit(t, inst, prim, u, v, nq, front) takes each closer
+// accepted hit, t.tmax already lowered to it. Shadow rays multiply the
+// transparent crossings' Fresnel transmission into trProd and add their
+// signed optical depth into tau.
+template <bool SHADOW, bool COUNT, class Sink>
+__device__ __forceinline__ int binTravStep(BinTrav& t, TravStack& stack, const SdLaunch& lp,
+                                           Sink& sink, float& trProd, float3& tau,
+                                           TraceCount* cnt) {
+  const float tmin = 0.0f;
+  if (COUNT) countWarp(cnt, cnt->travIters, cnt->travLanes);
+  if (t.cur >= 0) {
+    BvhNode nd = loadNode(lp.nodes, t.cur);
+    if (COUNT) cnt->boxTests += 2;
+    float ta, tb;
+    bool ha, hb;
+    boxPair(nd, t.oi, t.id, tmin, t.tmax, ta, tb, ha, hb);
+    if (ha && hb) {
+      int first = nd.link.x, second = nd.link.y;
+      if (tb < ta) {
+        first = nd.link.y;
+        second = nd.link.x;
+      }
+      if (t.sp < kStackSize) stack[t.sp++] = second;
+      t.cur = first;
+    } else if (ha) {
+      t.cur = nd.link.x;
+    } else if (hb) {
+      t.cur = nd.link.y;
+    } else {
+      return binTravPop(t, stack, sink);
+    }
+    return kTravMore;
+  }
+  if (t.cur == kPop) return binTravPop(t, stack, sink);  // a walk with no TLAS
+  // Leaf: ~cur = start << 3 | (count - 1).
+  const int code = ~t.cur;
+  const int start = code >> 3;
+  const int count = (code & 7) + 1;
+  if (!t.inBlas) {
+    // TLAS leaves hold exactly one instance; ro, rd are the world ray here.
+    const SdInstance& in = lp.inst[start];
+    float3 o2 = xfPoint(in.w2o, t.ro), d2 = xfVec(in.w2o, t.rd);
+    if (in.kind == GK_MESH) {
+      if (COUNT) cnt->blasEntries++;
+      // Always room: the scene build bounds TLAS + BLAS depth by the stack.
+      if (t.sp < kStackSize) {
+        stack[t.sp++] = kToTlas;
+        t.inBlas = true;
+        t.curInst = start;
+        t.ro = o2;
+        t.rd = d2;
+        t.id = v3(safeInv(d2.x), safeInv(d2.y), safeInv(d2.z));
+        t.oi = o2 * t.id;
+        t.wr = wtSetup(d2);
+        t.cur = lp.meshes[in.mesh].root;
+        return kTravMore;
+      }
+      return binTravPop(t, stack, sink);
+    }
+    if (COUNT) cnt->quadTests++;
+    QHits qh = hitQuadric(in.kind, o2, d2, tmin, t.tmax);
+    for (int k = 0; k < qh.n; k++) {
+      const QHit& q = qh.h[k];
+      if (q.t >= t.tmax) continue;
+      bool front = dot(q.n, d2) < 0.0f;
+      if ((in.flags & kInstMasked) && !faceAccepts(lp, in, front, q.u, q.v)) continue;
+      if (SHADOW) {
+        if (!(in.flags & kInstTransmissive)) return kTravOccluded;
+        uint16_t mid = front ? (uint16_t)(in.mats & 0xFFFF) : (uint16_t)(in.mats >> 16);
+        ShadePt spt = quadShade(in, q.n, q.u, q.v, sink.worldDir());
+        if (!shadowCross(lp, spt, mid, q.t, sink.worldDir(), trProd, tau)) return kTravOccluded;
+      } else {
+        t.tmax = q.t;
+        sink.hit(q.t, start, 0, q.u, q.v, q.n, front);
+      }
+    }
+    return binTravPop(t, stack, sink);
+  }
+  // BLAS leaf: triangles in object space of curInst.
+  for (int k = 0; k < count; k++) {
+    const float4* tp = lp.tris + 3 * (size_t)(start + k);
+    float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+    if (COUNT) cnt->triTests++;
+    float tt, b1, b2;
+    float3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
+    if (!wtHit(t.wr, t.ro, p0, p1, p2, tmin, t.tmax, tt, b1, b2)) continue;
+    const int prim = __float_as_int(a.w);
+    const SdInstance& in = lp.inst[t.curInst];
+    if (!(in.flags & (kInstMasked | kInstTransmissive))) {
+      if (SHADOW) return kTravOccluded;
+      t.tmax = tt;
+      sink.hit(tt, t.curInst, prim, b1, b2, v3(0.0f), dot(cross(p1 - p0, p2 - p0), t.rd) < 0.0f);
+      continue;
+    }
+    ShadePt spt = triShade(lp, in, prim, b1, b2, sink.worldDir());
+    if ((in.flags & kInstMasked) && !faceAccepts(lp, in, spt.front, spt.u, spt.v)) continue;
+    if (SHADOW) {
+      if (!(in.flags & kInstTransmissive)) return kTravOccluded;
+      uint16_t mid = spt.front ? (uint16_t)(in.mats & 0xFFFF) : (uint16_t)(in.mats >> 16);
+      if (!shadowCross(lp, spt, mid, tt, sink.worldDir(), trProd, tau)) return kTravOccluded;
+    } else {
+      t.tmax = tt;
+      sink.hit(tt, t.curInst, prim, b1, b2, v3(0.0f), spt.front);
+    }
+  }
+  return binTravPop(t, stack, sink);
+}
+
+// Sink of a single traversal call: the world ray in registers, the closest
+// hit into a TraceHit.
+struct RegisterSink {
+  float3 O, D;
+  TraceHit* out;
+  bool found;
+  __device__ __forceinline__ void world(float3& ro, float3& rd) const {
+    ro = O;
+    rd = D;
+  }
+  __device__ __forceinline__ float3 worldDir() const { return D; }
+  __device__ __forceinline__ void hit(float t, int inst, int prim, float u, float v, float3 nq,
+                                      bool front) {
+    found = true;
+    out->t = t;
+    out->inst = inst;
+    out->prim = prim;
+    out->u = u;
+    out->v = v;
+    out->nq = nq;
+    out->front = front;
+  }
+};
+
 // SHADOW = false: closest accepted hit, returns whether one was found.
 // SHADOW = true: returns false when occluded, else accumulates the
 // transparent-crossing terms into trProd / tau.
 template <bool SHADOW, bool COUNT = false>
 __device__ SDB_TRAVERSE_INLINE bool traverse(const SdLaunch& lp, float3 O, float3 D, float tmax,
-                                         TraceHit& hit, float& trProd, float3& tau,
-                                         TraceCount* cnt = nullptr) {
+                                             TraceHit& hit, float& trProd, float3& tau,
+                                             TraceCount* cnt = nullptr) {
   if (COUNT) cnt->traces++;
   if (lp.numInstances == 0) return SHADOW;
-  int stack[kStackSize];
-  int sp = 0;
-  const BvhNode* nodes = lp.nodes;
-  const float tmin = 0.0f;
-
-  float3 ro = O, rd = D;
-  float3 id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
-  float3 oi = ro * id;
-  WtRay wr;
-  bool inBlas = false;
-  int curInst = -1;
-  bool found = false;
-  int cur = lp.tlasRoot;
-
-  while (true) {
-    if (COUNT) countWarp(cnt, cnt->travIters, cnt->travLanes);
-    if (cur >= 0) {
-      BvhNode nd = loadNode(nodes, cur);
-      if (COUNT) cnt->boxTests += 2;
-      float ta, tb;
-      bool ha, hb;
-      boxPair(nd, oi, id, tmin, tmax, ta, tb, ha, hb);
-      if (ha && hb) {
-        int first = nd.link.x, second = nd.link.y;
-        if (tb < ta) {
-          first = nd.link.y;
-          second = nd.link.x;
-        }
-        if (sp < kStackSize) stack[sp++] = second;
-        cur = first;
-      } else if (ha) {
-        cur = nd.link.x;
-      } else if (hb) {
-        cur = nd.link.y;
-      } else {
-        cur = kPop;
-      }
-      continue;
-    }
-    if (cur == kPop) {
-      if (sp == 0) break;
-      cur = stack[--sp];
-      if (cur == kToTlas) {
-        inBlas = false;
-        ro = O;
-        rd = D;
-        id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
-        oi = ro * id;
-        cur = kPop;
-      }
-      continue;
-    }
-    // Leaf: ~cur = start << 3 | (count - 1).
-    int code = ~cur;
-    int start = code >> 3;
-    int count = (code & 7) + 1;
-    cur = kPop;
-    if (!inBlas) {
-      // TLAS leaves hold exactly one instance.
-      const SdInstance& in = lp.inst[start];
-      float3 o2 = xfPoint(in.w2o, O), d2 = xfVec(in.w2o, D);
-      if (in.kind == GK_MESH) {
-        if (COUNT) cnt->blasEntries++;
-        if (sp < kStackSize) {
-          stack[sp++] = kToTlas;
-          inBlas = true;
-          curInst = start;
-          ro = o2;
-          rd = d2;
-          id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
-          oi = ro * id;
-          wr = wtSetup(rd);
-          cur = lp.meshes[in.mesh].root;
-        }
-        continue;
-      }
-      if (COUNT) cnt->quadTests++;
-      QHits qh = hitQuadric(in.kind, o2, d2, tmin, tmax);
-      for (int k = 0; k < qh.n; k++) {
-        const QHit& q = qh.h[k];
-        if (q.t >= tmax) continue;
-        bool front = dot(q.n, d2) < 0.0f;
-        if ((in.flags & kInstMasked) && !faceAccepts(lp, in, front, q.u, q.v)) continue;
-        if (SHADOW) {
-          if (!(in.flags & kInstTransmissive)) return false;
-          uint16_t mid = front ? (uint16_t)(in.mats & 0xFFFF) : (uint16_t)(in.mats >> 16);
-          ShadePt spt = quadShade(in, q.n, q.u, q.v, D);
-          if (!shadowCross(lp, spt, mid, q.t, D, trProd, tau)) return false;
-        } else {
-          tmax = q.t;
-          found = true;
-          hit.t = q.t;
-          hit.inst = start;
-          hit.prim = 0;
-          hit.u = q.u;
-          hit.v = q.v;
-          hit.nq = q.n;
-          hit.front = front;
-        }
-      }
-      continue;
-    }
-    // BLAS leaf: triangles in object space of curInst.
-    for (int k = 0; k < count; k++) {
-      const float4* tp = lp.tris + 3 * (size_t)(start + k);
-      float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-      if (COUNT) cnt->triTests++;
-      float t, b1, b2;
-      float3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
-      if (!wtHit(wr, ro, p0, p1, p2, tmin, tmax, t, b1, b2)) continue;
-      int prim = __float_as_int(a.w);
-      const SdInstance& in = lp.inst[curInst];
-      bool needFace = (in.flags & (kInstMasked | kInstTransmissive)) != 0;
-      if (!needFace) {
-        if (SHADOW) return false;
-        tmax = t;
-        found = true;
-        hit.t = t;
-        hit.inst = curInst;
-        hit.prim = prim;
-        hit.u = b1;
-        hit.v = b2;
-        hit.front = dot(cross(p1 - p0, p2 - p0), rd) < 0.0f;
-        continue;
-      }
-      ShadePt spt = triShade(lp, in, prim, b1, b2, D);
-      if ((in.flags & kInstMasked) && !faceAccepts(lp, in, spt.front, spt.u, spt.v)) continue;
-      if (SHADOW) {
-        if (!(in.flags & kInstTransmissive)) return false;
-        uint16_t mid = spt.front ? (uint16_t)(in.mats & 0xFFFF) : (uint16_t)(in.mats >> 16);
-        if (!shadowCross(lp, spt, mid, t, D, trProd, tau)) return false;
-      } else {
-        tmax = t;
-        found = true;
-        hit.t = t;
-        hit.inst = curInst;
-        hit.prim = prim;
-        hit.u = b1;
-        hit.v = b2;
-        hit.front = spt.front;
-      }
-    }
-  }
-  return SHADOW ? true : found;
+  BinTrav t;
+  TravStack stack;
+  binTravStart(t, lp, O, D, tmax);
+  RegisterSink sink{O, D, &hit, false};
+  int r;
+  do {
+    r = binTravStep<SHADOW, COUNT>(t, stack, lp, sink, trProd, tau, cnt);
+  } while (r == kTravMore);
+  if (SHADOW) return r == kTravDone;
+  return sink.found;
 }
-
 
 #endif
 }  // namespace sdb

@@ -350,26 +350,37 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
   addRays<SERVE ? kWfServe : 0>(rays);
 }
 #else
+// Sink of the trace stage's walks (binTravStep, sd_trace.cuh): closer hits go
+// straight to the slot's hit record and the world ray is re-read from the
+// slot when a walk leaves a BLAS, so neither stays in registers.
+struct PoolSink {
+  const WfPool& pool;
+  int slot;
+  __device__ __forceinline__ void world(float3& ro, float3& rd) const {
+    ro = pool.paths[slot].v.o;
+    rd = pool.paths[slot].v.d;
+  }
+  __device__ __forceinline__ float3 worldDir() const { return pool.paths[slot].v.d; }
+  __device__ __forceinline__ void hit(float t, int inst, int prim, float u, float v, float3 nq,
+                                      bool front) const {
+    putHit(pool.hits[slot], t, inst, prim, u, v, nq, front);
+  }
+};
+
 template <bool SERVE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetch(int in) {
   const WfPool& pool = c_pool;
   const unsigned n = pool.counts[in];
   const unsigned full = 0xFFFFFFFFu;
   const unsigned ltMask = (1u << (threadIdx.x & 31)) - 1u;
-  const BvhNode* nodes = c_wlp.nodes;
   int job = 0;  // SERVE: the lane's job slot
-  const float tmin = 0.0f;
   unsigned long long rays = 0;
   int slot = -1;
   bool exhausted = false;  // warp-uniform
-  // The current space's ray (world in the TLAS, object space in a BLAS); the
-  // world ray is re-read from the slot when a BLAS is left.
-  float3 ro = v3(0.0f), rd = v3(0.0f), id = v3(0.0f), oi = v3(0.0f);
-  WtRay wr;
-  float tmax = 0.0f;  // the closest accepted hit so far (1e16: none)
-  bool inBlas = false;
-  int curInst = -1, cur = kPop, sp = 0;
-  int stack[kStackSize];
+  BinTrav t;
+  TravStack stack;
+  float trUnused = 1.0f;
+  float3 tauUnused = v3(0.0f);
   while (true) {
     const unsigned idle = __ballot_sync(full, slot < 0);
     if (!exhausted && (idle == full || __popc(idle) >= SDB_WF_FETCH_IDLE)) {
@@ -384,16 +395,8 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
           slot = pool.lists[in][i];
           if (SERVE) job = pool.jobs[slot];
           const SdLaunch& jl = SERVE ? c_wjobs[job] : c_wlp;
-          ro = pool.paths[slot].v.o;
-          rd = pool.paths[slot].v.d;
-          id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
-          oi = ro * id;
-          tmax = 1e16f;
+          binTravStart(t, jl, pool.paths[slot].v.o, pool.paths[slot].v.d, 1e16f);
           pool.hits[slot].v.inst = -1;  // a miss until a hit is stored
-          inBlas = false;
-          curInst = -1;
-          sp = 0;
-          cur = jl.numInstances > 0 ? jl.tlasRoot : kPop;
         }
       }
     }
@@ -403,99 +406,10 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
     }
     if (slot < 0) continue;
     const SdLaunch& lp = SERVE ? c_wjobs[job] : c_wlp;
-    if (cur >= 0) {
-      BvhNode nd = loadNode(SERVE ? lp.nodes : nodes, cur);
-      float ta, tb;
-      bool ha, hb;
-      boxPair(nd, oi, id, tmin, tmax, ta, tb, ha, hb);
-      if (ha && hb) {
-        int first = nd.link.x, second = nd.link.y;
-        if (tb < ta) {
-          first = nd.link.y;
-          second = nd.link.x;
-        }
-        if (sp < kStackSize) stack[sp++] = second;
-        cur = first;
-      } else if (ha) {
-        cur = nd.link.x;
-      } else if (hb) {
-        cur = nd.link.y;
-      } else {
-        cur = kPop;
-      }
-      continue;
-    }
-    if (cur == kPop) {
-      if (sp == 0) {  // ray done: its closest hit is already in the slot
-        rays++;
-        slot = -1;
-        continue;
-      }
-      cur = stack[--sp];
-      if (cur == kToTlas) {
-        inBlas = false;
-        ro = pool.paths[slot].v.o;
-        rd = pool.paths[slot].v.d;
-        id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
-        oi = ro * id;
-        cur = kPop;
-      }
-      continue;
-    }
-    // Leaf: ~cur = start << 3 | (count - 1).
-    const int code = ~cur;
-    const int start = code >> 3;
-    const int count = (code & 7) + 1;
-    cur = kPop;
-    if (!inBlas) {
-      // TLAS leaves hold exactly one instance.
-      const SdInstance& inst = lp.inst[start];
-      float3 o2 = xfPoint(inst.w2o, ro), d2 = xfVec(inst.w2o, rd);  // ro, rd: world here
-      if (inst.kind == GK_MESH) {
-        if (sp < kStackSize) {
-          stack[sp++] = kToTlas;
-          inBlas = true;
-          curInst = start;
-          ro = o2;
-          rd = d2;
-          id = v3(safeInv(rd.x), safeInv(rd.y), safeInv(rd.z));
-          oi = ro * id;
-          wr = wtSetup(rd);
-          cur = lp.meshes[inst.mesh].root;
-        }
-        continue;
-      }
-      QHits qh = hitQuadric(inst.kind, o2, d2, tmin, tmax);
-      for (int k = 0; k < qh.n; k++) {
-        const QHit& q = qh.h[k];
-        if (q.t >= tmax) continue;
-        bool front = dot(q.n, d2) < 0.0f;
-        if ((inst.flags & kInstMasked) && !faceAccepts(lp, inst, front, q.u, q.v)) continue;
-        tmax = q.t;
-        putHit(pool.hits[slot], q.t, start, 0, q.u, q.v, q.n, front);
-      }
-      continue;
-    }
-    // BLAS leaf: triangles in object space of curInst.
-    for (int k = 0; k < count; k++) {
-      const float4* tp = lp.tris + 3 * (size_t)(start + k);
-      float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-      float t, b1, b2;
-      float3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
-      if (!wtHit(wr, ro, p0, p1, p2, tmin, tmax, t, b1, b2)) continue;
-      int prim = __float_as_int(a.w);
-      const SdInstance& inst = lp.inst[curInst];
-      bool needFace = (inst.flags & (kInstMasked | kInstTransmissive)) != 0;
-      bool front;
-      if (!needFace) {
-        front = dot(cross(p1 - p0, p2 - p0), rd) < 0.0f;
-      } else {
-        ShadePt spt = triShade(lp, inst, prim, b1, b2, pool.paths[slot].v.d);
-        if ((inst.flags & kInstMasked) && !faceAccepts(lp, inst, spt.front, spt.u, spt.v)) continue;
-        front = spt.front;
-      }
-      tmax = t;
-      putHit(pool.hits[slot], t, curInst, prim, b1, b2, v3(0.0f), front);
+    PoolSink sink{pool, slot};
+    if (binTravStep<false, false>(t, stack, lp, sink, trUnused, tauUnused, nullptr) == kTravDone) {
+      rays++;  // its closest hit is already in the slot
+      slot = -1;
     }
   }
   addRays<SERVE ? kWfServe : 0>(rays);
