@@ -75,6 +75,34 @@ SDB_HD float fbm3(float3 p, unsigned seed) {
   return sum;
 }
 
+// valueNoise at a point with p.y == 0: the y fade weight is exactly 0, so
+// each y lerp returns its lower end unchanged (a + (b - a) * 0 == a for the
+// finite lattice values) and the four lattice values at iy + 1 never count.
+// The same value from half the hashes.
+SDB_HD float valueNoiseY0(float3 p, unsigned seed) {
+  float fx = floorf(p.x), fz = floorf(p.z);
+  int ix = (int)fx, iz = (int)fz;
+  float tx = p.x - fx, tz = p.z - fz;
+  tx = tx * tx * (3.0f - 2.0f * tx);
+  tz = tz * tz * (3.0f - 2.0f * tz);
+  float c000 = latticeValue(ix, 0, iz, seed), c100 = latticeValue(ix + 1, 0, iz, seed);
+  float c001 = latticeValue(ix, 0, iz + 1, seed), c101 = latticeValue(ix + 1, 0, iz + 1, seed);
+  float x00 = c000 + (c100 - c000) * tx;
+  float x01 = c001 + (c101 - c001) * tx;
+  return x00 + (x01 - x00) * tz;
+}
+
+// fbm3 of a point on the plane y == 0 (the wave height field): the first
+// octave through valueNoiseY0, the others as in fbm3.
+SDB_HD float fbm3Y0(float3 p, unsigned seed) {
+  float sum = 0.5f * valueNoiseY0(p, seed);
+  p = 2.03f * p + v3(11.7f, 5.3f, 7.9f);
+  sum += 0.25f * valueNoise(p, seed + 101u);
+  p = 2.03f * p + v3(11.7f, 5.3f, 7.9f);
+  sum += 0.125f * valueNoise(p, seed + 202u);
+  return sum;
+}
+
 // Wave normal from an fBm height field over world xz by central differences;
 // falls back to ns when the perturbed normal would face away from wo.
 // (device/noise.cuh:67-79)
@@ -82,8 +110,8 @@ SDB_COLD float3 waveNormal(float3 x, float3 ns, float3 wo, float amp, float freq
   const unsigned seed = 1337u;
   const float e = 0.05f;
   float3 p = v3(x.x * freq, 0.0f, x.z * freq);
-  float hx1 = fbm3(p + v3(e, 0.0f, 0.0f), seed), hx0 = fbm3(p - v3(e, 0.0f, 0.0f), seed);
-  float hz1 = fbm3(p + v3(0.0f, 0.0f, e), seed), hz0 = fbm3(p - v3(0.0f, 0.0f, e), seed);
+  float hx1 = fbm3Y0(p + v3(e, 0.0f, 0.0f), seed), hx0 = fbm3Y0(p - v3(e, 0.0f, 0.0f), seed);
+  float hz1 = fbm3Y0(p + v3(0.0f, 0.0f, e), seed), hz0 = fbm3Y0(p - v3(0.0f, 0.0f, e), seed);
   float dhdx = (hx1 - hx0) / (2.0f * e);
   float dhdz = (hz1 - hz0) / (2.0f * e);
   float side = ns.y >= 0.0f ? 1.0f : -1.0f;
@@ -102,9 +130,15 @@ SDB_HD void flameAt(const SdFlame& fl, float3 p, float& sigma, float3& eps) {
   float rx = p.x - fl.base.x, rz = p.z - fl.base.z;
   float d = sqrtf(rx * rx + rz * rz) / fl.radius;
   float prof = 3.2f * sqrtf(h) * powf(1.0f - h, 1.55f);
+  const float dp = d / fmaxf(prof, 1e-3f);
+  // The noise term n - 0.45 is at least -0.45 (fBm is non-negative), so where
+  // dp - 0.45 already reaches the mask's outer edge (1) the mask is 0 for
+  // every noise value: return the empty medium without evaluating the noise
+  // (the same result: rounding is monotonic).
+  if (dp - 0.45f >= 1.0f) return;
   float3 q = v3(rx / fl.radius, (p.y - fl.base.y) / fl.radius * 0.32f, rz / fl.radius);
   float n = fbm3(q * fl.noiseScale, fl.seed);
-  float dd = d / fmaxf(prof, 1e-3f) + (n - 0.45f) * 1.0f;
+  float dd = dp + (n - 0.45f) * 1.0f;
   float mask = smoothRamp(1.0f, 0.62f, dd) * smoothRamp(0.0f, 0.12f, h);
   if (mask <= 0.0f) return;
   sigma = fl.sigma * mask;
