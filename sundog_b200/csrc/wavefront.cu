@@ -167,12 +167,18 @@ __device__ __forceinline__ void putHit(PoolSlot<TraceHit>& s, float t, int inst,
   p[2] = make_float4(__int_as_float(front ? 1 : 0), 0.0f, 0.0f, 0.0f);
 }
 
-// Node visits a lane may take in a row inside one round of the fetch loop
-// (config 1 / config 0, Mrays/s: 1 visit 1,351 / 2,648; 4: 1,459 / 2,697;
-// 8: 1,497 / 2,723; 16: 1,512 / 2,726; 64: 1,499 / 2,709; letting leaves
-// continue the run too, 16 steps: 1,405 / 2,692).
+// Steps a lane may take in a row inside one round of the fetch loop, and
+// the fewest lanes still descending that keep the warp in the run (config 1
+// / config 0, Mrays/s; while any lane descends: 1 step 1,351 / 2,648; 4:
+// 1,459 / 2,697; 8: 1,497 / 2,723; 16: 1,512 / 2,726; 64: 1,499 / 2,709;
+// letting leaves continue the run too, 16 steps: 1,405 / 2,692; 16 steps
+// while at least 2 / 4 / 8 / 12 lanes descend: 1,555 / 2,713, 1,568 /
+// 2,718, 1,559 / 2,655, 1,525 / 2,680).
 #ifndef SDB_WF_INNER
 #define SDB_WF_INNER 16
+#endif
+#ifndef SDB_WF_INNER_MIN
+#define SDB_WF_INNER_MIN 4
 #endif
 // Idle lanes a warp gathers before it fetches new rays (measured on the
 // instancing frame: 894 Mrays/s at 24, 869 with a grid-stride loop, 752 when
@@ -411,18 +417,21 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfTraceFetc
       if (exhausted) break;
       continue;
     }
-    if (slot < 0) continue;
+    // One step for every lane with a ray; then lanes that landed on an
+    // inner node keep descending (the while-while loop of Aila and Laine
+    // 2009 inside the dynamic-fetch loop) while at least SDB_WF_INNER_MIN of
+    // the warp's lanes do so, up to SDB_WF_INNER steps, before the warp
+    // meets again at the fetch vote; lanes at a leaf wait for the next round.
     const SdLaunch& lp = SERVE ? c_wjobs[job] : c_wlp;
     PoolSink sink{pool, slot};
-    // A lane that lands on an inner node keeps descending, up to
-    // SDB_WF_INNER node visits, before the warp meets again at the fetch
-    // vote; a lane at a leaf waits for the next round (the while-while loop
-    // of Aila and Laine 2009 inside the dynamic-fetch loop).
-    int r, k = 0;
-    do {
-      r = binTravStep<false, false>(t, stack, lp, sink, trUnused, tauUnused, nullptr);
-    } while (r == kTravMore && t.cur >= 0 && ++k < SDB_WF_INNER);
-    if (r == kTravDone) {
+    int r = kTravMore;
+    bool go = slot >= 0;
+    for (int k = 1;; k++) {
+      if (go) r = binTravStep<false, false>(t, stack, lp, sink, trUnused, tauUnused, nullptr);
+      go = slot >= 0 && r == kTravMore && t.cur >= 0;
+      if (k >= SDB_WF_INNER || __popc(__ballot_sync(full, go)) < SDB_WF_INNER_MIN) break;
+    }
+    if (slot >= 0 && r == kTravDone) {
       rays++;  // its closest hit is already in the slot
       slot = -1;
     }
