@@ -476,8 +476,12 @@ class Server {
     std::lock_guard<std::mutex> launchLock(deviceLaunchLock());
     std::vector<SdLaunch> table(kMaxServeJobs);
     std::memset(table.data(), 0, table.size() * sizeof(SdLaunch));
+    int maxInstances = 0;
     for (size_t k = 0; k < slots.size(); k++)
-      if (slots[k]) table[k] = slots[k]->lp;
+      if (slots[k]) {
+        table[k] = slots[k]->lp;
+        maxInstances = std::max(maxInstances, slots[k]->lp.numInstances);
+      }
     // Both engines fold through ptServeFold, which reads the megakernel's
     // table; the wavefront stages read their own.
     cudaCheck(serveSetJobs(table.data(), st), "job table");
@@ -495,7 +499,7 @@ class Server {
     b.sampleL = (float4*)scratch.ptr;
     cudaCheck(cudaEventRecord(ev0, st), "event");
     if (wf) {
-      wfRenderBatch(b, *wf, st);
+      wfRenderBatch(b, *wf, st, maxInstances);
       cudaCheck(serveFold(b, st), "serve fold");
     } else {
       cudaCheck(serveLaunch(b, grid, st), "serve launch");

@@ -465,6 +465,8 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeA(in
   addRays<GUIDE>(rays);
 }
 
+// Shadow rays, one per thread to the end of its walk (grid-stride over the
+// shadow list).
 template <int GUIDE>
 __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfShadow() {
   const WfPool& pool = c_pool;
@@ -477,6 +479,88 @@ __global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfShadow() 
     pool.trs[slot] = make_float4(tr.x, tr.y, tr.z, 0.0f);
   }
 }
+
+#if !SDB_WIDE_BVH
+// Sink of the shadow stage's walks: the world ray is the slot's queued
+// shadow ray, re-read when a walk leaves a BLAS.
+struct ShadowSink {
+  const WfPool& pool;
+  int slot;
+  __device__ __forceinline__ void world(float3& ro, float3& rd) const {
+    ro = pool.verts[slot].v.so;
+    rd = pool.verts[slot].v.wi;
+  }
+  __device__ __forceinline__ float3 worldDir() const { return pool.verts[slot].v.wi; }
+  __device__ __forceinline__ void hit(float, int, int, float, float, float3, bool) const {}
+};
+
+// Shadow rays with the trace stage's dynamic fetch (counter counts[4]) and
+// node-descent runs: the walk and transmittance of shadowTransmittance, many
+// rays interleaved per warp. Faster than wfShadow where walks are long and
+// uneven (config 1, 1024 instances: 29.3 -> 24.5 ms per frame), slower on
+// small scenes (config 0: 2,730 -> 2,672 Mrays/s; config 2: 113.7 -> 122.2
+// ms), so renders choose by instance count (kShadowFetchInstances).
+template <int GUIDE>
+__global__ void __launch_bounds__(kRenderBlock, SDB_WF_TRACE_BLOCKS) wfShadowFetch() {
+  const WfPool& pool = c_pool;
+  const unsigned n = pool.counts[2];
+  const unsigned full = 0xFFFFFFFFu;
+  const unsigned ltMask = (1u << (threadIdx.x & 31)) - 1u;
+  int slot = -1;
+  bool exhausted = false;  // warp-uniform
+  BinTrav t;
+  TravStack stack;
+  float trProd = 1.0f;
+  float3 tau = v3(0.0f);
+  while (true) {
+    const unsigned idle = __ballot_sync(full, slot < 0);
+    if (!exhausted && (idle == full || __popc(idle) >= SDB_WF_FETCH_IDLE)) {
+      const int leader = __ffs(idle) - 1;
+      unsigned base = 0;
+      if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&pool.counts[4], (unsigned)__popc(idle));
+      base = __shfl_sync(full, base, leader);
+      if (base + __popc(idle) >= n) exhausted = true;
+      if (slot < 0) {
+        unsigned i = base + __popc(idle & ltMask);
+        if (i < n) {
+          slot = pool.shadowList[i];
+          const Vertex& v = pool.verts[slot].v;
+          binTravStart(t, slotLaunch<GUIDE>(slot), v.so, v.wi, v.tmaxS);
+          trProd = 1.0f;
+          tau = v3(0.0f);
+        }
+      }
+    }
+    if (__ballot_sync(full, slot >= 0) == 0) {
+      if (exhausted) break;
+      continue;
+    }
+    const SdLaunch& lp = slotLaunch<GUIDE>(slot >= 0 ? slot : 0);
+    ShadowSink sink{pool, slot};
+    int r = kTravMore;
+    bool go = slot >= 0;
+    for (int k = 1;; k++) {
+      if (go) r = binTravStep<true, false>(t, stack, lp, sink, trProd, tau, nullptr);
+      go = slot >= 0 && r == kTravMore && t.cur >= 0;
+      if (k >= SDB_WF_INNER || __popc(__ballot_sync(full, go)) < SDB_WF_INNER_MIN) break;
+    }
+    if (slot >= 0 && r != kTravMore) {
+      float3 tr = v3(0.0f);
+      if (r == kTravDone) {
+        tau = v3(fmaxf(0.0f, tau.x), fmaxf(0.0f, tau.y), fmaxf(0.0f, tau.z));
+        tr = v3(trProd);
+        if (hmax(tau) > 0.0f) tr = tr * vexp(-tau);
+      }
+      pool.trs[slot] = make_float4(tr.x, tr.y, tr.z, 0.0f);
+      slot = -1;
+    }
+  }
+}
+#else
+// The 8-wide build traces shadow rays one per thread.
+template <int GUIDE>
+__global__ void wfShadowFetch() {}
+#endif
 
 // GUIDE & kGuideSample: the BSDF sample by MIS with the learned guide
 // (sd_guide.cuh; the mixture table is in the launch block). GUIDE &
@@ -538,7 +622,7 @@ void WfBuffers::ensure(int slots) {
   list1.alloc((size_t)slots * sizeof(int));
   shadow.alloc((size_t)slots * sizeof(int));
   jobs.alloc((size_t)slots);
-  if (!counts.ptr) counts.alloc(4 * sizeof(unsigned));
+  if (!counts.ptr) counts.alloc(8 * sizeof(unsigned));
   if (!hostCount) cudaCheck(cudaMallocHost((void**)&hostCount, 4 * sizeof(unsigned)), "pinned count");
   cap = slots;
   gridTrace = gridFor(wfTraceFetch<false>);
@@ -604,13 +688,17 @@ size_t wfSlotBytes() {
 // One iteration's stage kernels for mode GUIDE (guide bits, or kWfServe).
 // With `timed`, events ev[1..5] bracket the four stage launches.
 template <int GUIDE>
-static void wfIteration(const WfBuffers& b, cudaStream_t st, int cur, int nxt, bool timed) {
+static void wfIteration(const WfBuffers& b, cudaStream_t st, int cur, int nxt, bool timed,
+                        bool shadowFetch) {
   if (timed) cudaEventRecord(b.ev[1], st);
   wfTraceFetch<(GUIDE & kWfServe) != 0><<<b.gridTrace, kRenderBlock, 0, st>>>(cur);
   if (timed) cudaEventRecord(b.ev[2], st);
   wfShadeA<GUIDE><<<b.gridShadeA, kRenderBlock, 0, st>>>(cur, nxt);
   if (timed) cudaEventRecord(b.ev[3], st);
-  wfShadow<GUIDE><<<b.gridShadow, kRenderBlock, 0, st>>>();
+  if (shadowFetch && !SDB_WIDE_BVH)
+    wfShadowFetch<GUIDE><<<b.gridShadow, kRenderBlock, 0, st>>>();
+  else
+    wfShadow<GUIDE><<<b.gridShadow, kRenderBlock, 0, st>>>();
   if (timed) cudaEventRecord(b.ev[4], st);
   wfShadeB<GUIDE><<<b.gridShadeB, kRenderBlock, 0, st>>>(cur, nxt);
   if (timed) cudaEventRecord(b.ev[5], st);
@@ -626,7 +714,7 @@ static double evMs(cudaEvent_t a, cudaEvent_t b) {
 // iterations until no path is live (the launch block or batch is already in
 // constant memory). Returns the kernels launched.
 static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, int mode,
-                   WfStageTimes* times = nullptr) {
+                   bool shadowFetch, WfStageTimes* times = nullptr) {
   const bool timed = times != nullptr;
   if (timed && !b.ev[0])
     for (cudaEvent_t& e : b.ev) cudaCheck(cudaEventCreate(&e), "stage timing events");
@@ -667,13 +755,15 @@ static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, i
   for (int iter = 0;; iter++) {
     int nxt = 1 - cur;
     cudaCheck(cudaMemsetAsync(counts + nxt, 0, sizeof(unsigned), st), "wavefront counts");
-    cudaCheck(cudaMemsetAsync(counts + 2, 0, 2 * sizeof(unsigned), st), "wavefront counts");
+    cudaCheck(cudaMemsetAsync(counts + 2, 0, 3 * sizeof(unsigned), st), "wavefront counts");
     switch (mode) {
-      case 0: wfIteration<0>(b, st, cur, nxt, timed); break;
-      case kGuideSample: wfIteration<kGuideSample>(b, st, cur, nxt, timed); break;
-      case kGuideRecord: wfIteration<kGuideRecord>(b, st, cur, nxt, timed); break;
-      case kGuideSample | kGuideRecord: wfIteration<kGuideSample | kGuideRecord>(b, st, cur, nxt, timed); break;
-      default: wfIteration<kWfServe>(b, st, cur, nxt, timed); break;
+      case 0: wfIteration<0>(b, st, cur, nxt, timed, shadowFetch); break;
+      case kGuideSample: wfIteration<kGuideSample>(b, st, cur, nxt, timed, shadowFetch); break;
+      case kGuideRecord: wfIteration<kGuideRecord>(b, st, cur, nxt, timed, shadowFetch); break;
+      case kGuideSample | kGuideRecord:
+        wfIteration<kGuideSample | kGuideRecord>(b, st, cur, nxt, timed, shadowFetch);
+        break;
+      default: wfIteration<kWfServe>(b, st, cur, nxt, timed, shadowFetch); break;
     }
     cudaCheck(cudaGetLastError(), "wavefront stage");
     launches += 4;
@@ -705,7 +795,7 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide, WfSta
   if (guide & kGuideRecord) b.ensureTrails();
   cudaCheck(cudaMemcpyToSymbolAsync(c_wlp, &lp, sizeof lp, 0, cudaMemcpyHostToDevice, st),
             "wavefront launch block");
-  return runPool(b, st, lp.numPaths, guide, times);
+  return runPool(b, st, lp.numPaths, guide, lp.numInstances >= kShadowFetchInstances, times);
 }
 
 cudaError_t wfSetJobs(const SdLaunch* table, cudaStream_t st) {
@@ -713,10 +803,10 @@ cudaError_t wfSetJobs(const SdLaunch* table, cudaStream_t st) {
                                  cudaMemcpyHostToDevice, st);
 }
 
-int wfRenderBatch(const ServeBatch& batch, WfBuffers& b, cudaStream_t st) {
+int wfRenderBatch(const ServeBatch& batch, WfBuffers& b, cudaStream_t st, int maxInstances) {
   cudaCheck(cudaMemcpyToSymbolAsync(c_wbatch, &batch, sizeof batch, 0, cudaMemcpyHostToDevice, st),
             "wavefront batch");
-  return runPool(b, st, batch.numPaths, kWfServe);
+  return runPool(b, st, batch.numPaths, kWfServe, maxInstances >= kShadowFetchInstances);
 }
 
 }  // namespace sdb

@@ -83,8 +83,14 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide = 0,
 // launch blocks, host memory), and one batch of tile-passes rendered through
 // the pool into batch.sampleL at each path's id (the caller folds them).
 // Returns the kernels launched.
+// maxInstances: the largest instance count among the batch's scenes (picks
+// the shadow-ray kernel, as a render does by its own scene's count).
 struct ServeBatch;
 cudaError_t wfSetJobs(const SdLaunch* table, cudaStream_t st);
-int wfRenderBatch(const ServeBatch& batch, WfBuffers& b, cudaStream_t st);
+int wfRenderBatch(const ServeBatch& batch, WfBuffers& b, cudaStream_t st, int maxInstances = 0);
+
+// Scenes with at least this many instances trace their shadow rays with
+// dynamic fetch (wfShadowFetch), smaller ones one ray per thread (wfShadow).
+constexpr int kShadowFetchInstances = 64;
 
 }  // namespace sdb
