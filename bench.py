@@ -89,14 +89,18 @@ def parse_args():
                     help="path-tracing kernels: 0 automatic, 1 megakernel, 2 wavefront")
     ap.add_argument("--guiding", action="store_true",
                     help="learned-guiding equal-time relMSE line instead of Mrays/s")
-    ap.add_argument("--guide-spp", type=int, default=256)
-    ap.add_argument("--guide-width", type=int, default=2560)
-    ap.add_argument("--guide-height", type=int, default=1440)
+    ap.add_argument("--guide-spp", type=int, default=0,
+                    help="0: the guided scene's config (instancing 64, volumes 256)")
+    ap.add_argument("--guide-width", type=int, default=0,
+                    help="0: the guided scene's config (instancing 1920, volumes 2560)")
+    ap.add_argument("--guide-height", type=int, default=0,
+                    help="0: the guided scene's config (instancing 1080, volumes 1440)")
     ap.add_argument("--guide-ref-spp", type=int, default=16384)
     ap.add_argument("--guide-seeds", type=int, default=4)
-    ap.add_argument("--guide-scene", default="volumes", choices=["volumes", "instancing"],
-                    help="scene of the guiding line: flame / water / glass (volumes) or "
-                         "1024 instances under the sun-and-sky env map (instancing)")
+    ap.add_argument("--guide-scene", default="instancing", choices=["instancing", "volumes"],
+                    help="scene of the guiding line: the instancing config's 1024 instances "
+                         "under the sun-and-sky env map (the guiding config's scene), or the "
+                         "volumes config's flame / water / glass")
     ap.add_argument("--serving", action="store_true",
                     help="render-server line (Poisson jobs, p50/p99 latency) instead of Mrays/s")
     ap.add_argument("--serve-jobs", type=int, default=60)
@@ -641,8 +645,9 @@ def _relmse(img, ref):
 
 def run_guiding(args):
     """Learned guiding against a 16384-spp plain render of the same scene, by
-    default the flame / water / glass scene at its configured 2560x1440 and
-    256 spp (or the 1024-instance field under the sun-and-sky env map). Rare
+    default the instancing config's 1024-instance field under the sun-and-sky
+    env map at its 1920x1080 and 64 spp (or the volumes config's flame / water
+    / glass scene at its 2560x1440 and 256 spp). Rare
     high-energy paths make one render's relMSE too noisy to rank two methods:
     each method renders the frame with K seeds, and its error at a given time
     is its mean relMSE over the seeds scaled by (its render time / that time)
@@ -658,8 +663,9 @@ def run_guiding(args):
     from sundog_b200 import workloads
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    w, h = args.guide_width, args.guide_height
-    spp, ref_spp, seeds = args.guide_spp, args.guide_ref_spp, args.guide_seeds
+    dw, dh, dspp = (2560, 1440, 256) if args.guide_scene == "volumes" else (1920, 1080, 64)
+    w, h = args.guide_width or dw, args.guide_height or dh
+    spp, ref_spp, seeds = args.guide_spp or dspp, args.guide_ref_spp, args.guide_seeds
     ad = asset_dir()
     if args.guide_scene == "volumes":
         make = lambda n: workloads.volumes(ad, width=w, height=h, spp=n)
@@ -741,13 +747,16 @@ def run_guiding(args):
 # ---- serving: Poisson-arriving jobs, continuous batching ----------------------------------
 
 def run_serving(args):
-    """Render server under Poisson arrivals (rate 20/s, seed 5): each job
+    """Render server under Poisson arrivals (default rate 20/s, seed 5): each job
     draws a scene from the Cornell / instancing / volumes configs, a square
     resolution log-uniform in 256..2048 and spp log-uniform in 4..256, and is
     submitted at its arrival time; the server batches 64x64 tile-passes of all
     admitted jobs into each persistent launch. Reports p50 / p99 job latency
-    (submission -> film on the host) and aggregate Mrays/s over the run.
-    Prints one JSON line."""
+    (submission -> film on the host) and aggregate Mrays/s over the run; then
+    renders every job alone on a fresh server for its slowdown in the mix
+    (latency in the mix / latency alone), and gives the server's capacity
+    (camera paths per busy second) and the arrival rate it sustains (capacity
+    / mean paths per job). Prints one JSON line."""
     from sundog_b200 import serve, workloads
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
@@ -792,14 +801,29 @@ def run_serving(args):
         wall = time.perf_counter() - t0
         st = sv.stats()
     clocks = sampler.stop()
+    # Each job alone on an idle server, in arrival order: its latency in the
+    # mix over its latency alone is the slowdown the other jobs caused.
+    alone = []
+    with serve.Server(**cfg) as sv:
+        for i, (k, side, spp) in enumerate(work):
+            j = sv.submit(scenes[k], base_dir=ad, width=side, height=side, spp=spp, seed=1 + i)
+            try:
+                j.wait()
+            except serve.JobError:
+                pass
+            alone.append(j.last.latency_ms)
+            j.film = None
+    slow = np.array(lat) / np.maximum(np.array(alone), 1e-3)
+    capacity = st.paths / (st.busy_ms / 1e3) if st.busy_ms else None
+    mean_job_paths = float(np.mean([side * side * spp for _, side, spp in work]))
     paths_total = sum(side * side * spp for _, side, spp in work)
     line = {
         "metric": "serving: aggregate Mrays/s; p50/p99 job latency", "value": st.rays / wall / 1e6,
         "unit": "Mrays/s", "higher_is_better": True, "n_gpus": 1, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": "Poisson arrivals 20/s (seed 5) of Cornell / instancing / volumes "
+        "config": {"workload": "Poisson arrivals %g/s (seed 5) of Cornell / instancing / volumes "
                                "jobs, square 256..2048 px and 4..256 spp log-uniform, 64x64 "
-                               "tile-passes of 8 spp batched across jobs",
+                               "tile-passes of 8 spp batched across jobs" % args.serve_rate,
                    "jobs": n, "arrival_rate_per_s": args.serve_rate,
                    "max_jobs": sv.config.max_jobs,
                    "iteration_paths": sv.config.iteration_paths,
@@ -813,6 +837,17 @@ def run_serving(args):
         "busy_mrays_per_s": st.rays / (st.busy_ms / 1e3) / 1e6 if st.busy_ms else None,
         "samples_per_sec": st.paths / wall,
         "offered_paths_per_s": paths_total / float(arrivals[-1] if n > 1 else 1.0),
+        "capacity_paths_per_s": capacity,
+        "sustainable_rate_per_s": capacity / mean_job_paths if capacity else None,
+        "alone_latency_ms": {"p50": float(np.percentile(alone, 50)),
+                             "p99": float(np.percentile(alone, 99))},
+        "slowdown_vs_alone": {"p50": float(np.percentile(slow, 50)),
+                              "p99": float(np.percentile(slow, 99)),
+                              "max": float(np.max(slow))},
+        "per_job": [{"scene": ["cornell", "instancing", "volumes"][k], "side": side, "spp": spp,
+                     "arrival_ms": round(1e3 * float(at), 1), "latency_ms": round(l, 1),
+                     "queued_ms": round(q, 1), "alone_ms": round(a, 1)}
+                    for (k, side, spp), at, l, q, a in zip(work, arrivals, lat, queued, alone)],
         "iterations": st.iterations, "scenes_resident_at_end": st.scenes_resident,
         "clocks": clocks,
     }

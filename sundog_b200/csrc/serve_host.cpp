@@ -465,9 +465,35 @@ class Server {
       hItems[n++] = it;
       return true;
     };
-    for (size_t i = 0; i < act.size(); i++) add(i);  // one tile-pass each
+    // Shortest remaining work first: a job whose whole remaining work fits
+    // the budget, with room kept for one tile-pass of every job, goes in
+    // whole (every open tile with all its remaining samples as one item), so
+    // a small job finishes in this batch instead of taking one pass_spp pass
+    // of each tile per batch. The batch stays within iteration_paths.
+    std::vector<char> whole(act.size(), 0);
+    const uint64_t reserve = (uint64_t)act.size() * itemMax;
+    for (size_t i = 0; reserve < cfg.iteration_paths && i < act.size(); i++) {
+      ServeJob& j = *act[i];
+      uint64_t rem = 0;
+      int open = 0;
+      for (int t = 0; t < (int)j.tileNext.size(); t++)
+        if (j.tileNext[t] < j.spp) {
+          rem += (uint64_t)tileNpad(j, t) * (uint64_t)(j.spp - j.tileNext[t]);
+          open++;
+        }
+      if (rem == 0 || total + rem > cfg.iteration_paths - reserve || n + open > maxItems) continue;
+      ServeItem it;
+      while (nextTilePass(j, used[i], j.spp, it)) {
+        it.pathBegin = total;
+        total += (uint64_t)it.npad * it.sampleCount;
+        hItems[n++] = it;
+      }
+      whole[i] = 1;
+    }
+    for (size_t i = 0; i < act.size(); i++)  // one tile-pass each
+      if (!whole[i]) add(i);
     for (size_t i = 0; i < act.size(); i++)
-      while (total + itemMax <= cfg.iteration_paths && add(i)) {
+      while (!whole[i] && total + itemMax <= cfg.iteration_paths && add(i)) {
       }
     if (n == 0) return;
     // The job table and batch block live in per-device constant memory,
