@@ -76,7 +76,8 @@ struct ServeJob {
   Clock::time_point tSubmit, tAdmit, tEnd;
   // device side (server thread only)
   std::shared_ptr<const DeviceScene> dev;
-  DevBuf film;
+  DevBuf film;  // the device film (a pooled buffer may be larger than filmBytes)
+  uint64_t filmBytes = 0;
   SdLaunch lp{};
   int slot = -1;
   int tilesX = 0, tilesY = 0;
@@ -131,6 +132,7 @@ class Server {
     wfRelease(std::move(wf));
     for (auto& j : slots)
       if (j) j->film.release();
+    dropFilmPool();
     sceneCache.clear();
     if (hItems) cudaFreeHost(hItems);
     if (ev0) cudaEventDestroy(ev0);
@@ -268,8 +270,44 @@ class Server {
     cvDone.notify_all();
   }
 
+  // Films of finished jobs are kept for later jobs (up to kFilmPoolBytes):
+  // a job's admission then allocates no device memory, and a finished job
+  // frees none, so neither waits on the driver's allocator.
+  static constexpr uint64_t kFilmPoolBytes = 1ull << 30;
+  std::vector<DevBuf> filmPool;
+  uint64_t filmPoolBytes = 0;
+
+  void takeFilm(DevBuf& film, uint64_t bytes) {
+    int best = -1;
+    for (int k = 0; k < (int)filmPool.size(); k++)
+      if (filmPool[k].bytes >= bytes && (best < 0 || filmPool[k].bytes < filmPool[best].bytes))
+        best = k;
+    if (best < 0) {
+      film.alloc(bytes);
+      return;
+    }
+    filmPoolBytes -= filmPool[best].bytes;
+    film = std::move(filmPool[best]);
+    filmPool.erase(filmPool.begin() + best);
+  }
+
+  void returnFilm(DevBuf& film) {
+    if (!film.ptr) return;
+    if (filmPoolBytes + film.bytes > kFilmPoolBytes) {
+      film.release();
+      return;
+    }
+    filmPoolBytes += film.bytes;
+    filmPool.push_back(std::move(film));
+  }
+
+  void dropFilmPool() {
+    filmPool.clear();
+    filmPoolBytes = 0;
+  }
+
   void releaseJob(const std::shared_ptr<ServeJob>& j) {
-    j->film.release();
+    returnFilm(j->film);
     if (j->slot >= 0) slots[j->slot] = nullptr;
     j->slot = -1;
     if (j->dev) {
@@ -323,6 +361,7 @@ class Server {
       throw std::runtime_error("job needs more device memory than the device has");
     auto it = sceneCache.find(j->key);
     if (it == sceneCache.end()) {
+      dropFilmPool();
       evictScenes(filmBytes, freeB);
       cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
       if (freeB < filmBytes + cfg.reserve_bytes) return false;
@@ -332,6 +371,7 @@ class Server {
       cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
     }
     if (freeB < filmBytes + cfg.reserve_bytes) {
+      dropFilmPool();
       evictScenes(filmBytes, freeB);
       cudaCheck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
       if (freeB < filmBytes + cfg.reserve_bytes) {
@@ -345,7 +385,8 @@ class Server {
     it->second.users++;
     it->second.lastUse = ++useClock;
     j->dev = it->second.dev;
-    j->film.alloc(filmBytes);
+    takeFilm(j->film, filmBytes);
+    j->filmBytes = filmBytes;
     cudaCheck(cudaMemsetAsync(j->film.ptr, 0, filmBytes, st), "film reset");
     std::memset(&j->lp, 0, sizeof j->lp);
     fillRenderLaunch(j->lp, j->desc, j->desc.render);
@@ -555,7 +596,7 @@ class Server {
     for (auto& j : act) {
       if (j->pathsDone < j->pathsTotal) continue;
       if (j->hostFilm)
-        cudaCheck(cudaMemcpy(j->hostFilm, j->film.ptr, j->film.bytes, cudaMemcpyDeviceToHost),
+        cudaCheck(cudaMemcpy(j->hostFilm, j->film.ptr, j->filmBytes, cudaMemcpyDeviceToHost),
                   "film download");
       releaseJob(j);
       finish(j, SUNDOG_JOB_DONE, "");
