@@ -228,9 +228,9 @@ def ncu_traffic_per_path(engine=0):
     return float(m.group(1)) if m else None
 
 
-# Algorithmic bytes of one traversal step on a canonical binary BVH: 32 B per
-# child box tested (AABB 24 + link 8), 36 B per triangle, 48 B per quadric
-# (its affine), 64 B per instance transform entered.
+# Algorithmic bytes of the traversal on the BVH it walks (the library's 4-wide
+# nodes by default): 32 B per child box tested (AABB 24 + link 8), 36 B per
+# triangle, 48 B per quadric (its affine), 64 B per instance transform entered.
 def bytes_per_ray(c):
     total = 32.0 * c.box_tests + 36.0 * c.tri_tests + 48.0 * c.quadric_tests + 64.0 * c.blas_entries
     return total / max(c.rays, 1)
@@ -332,7 +332,8 @@ def stage_roofline(lib, ses, stream, flush, rad, shd, peak, workload):
         tr["frac_of_l2"] = tr["l2_gbps"] / l2
     out["iterations"] = t.iterations
     out["note"] = ("per-stage CUDA events in one extra render after the timed steps; "
-                   "bytes per ray on a binary BVH, radiance and shadow rays counted apart")
+                   "bytes per ray on the walked BVH (32 B per child box tested), radiance and "
+                   "shadow rays counted apart")
     return out
 
 
@@ -524,8 +525,9 @@ def run_ours(args):
                     "simt": {"traversal_lanes_per_iter": counts.trav_lanes / max(counts.trav_iters, 1),
                              "path_loop_lanes_per_iter": counts.loop_lanes / max(counts.loop_iters, 1),
                              "traversal_iters_per_ray": 32.0 * counts.trav_iters / max(counts.rays, 1)},
-                    "note": "algorithmic bytes on a binary BVH (32 B/box, 36 B/tri, 48 B/"
-                            "quadric, 64 B/instance) per chunk of samples (one persistent launch "
+                    "note": "algorithmic bytes on the walked BVH (4-wide nodes; 32 B per child "
+                            "box tested, 36 B/tri, 48 B/quadric, 64 B/instance) per chunk of "
+                            "samples (one persistent launch "
                             "or one wavefront pass) over its CUDA-event duration; the BVH (<4 MB) "
                             "and env tables are cache-resident, so HBM is a loose bound"}
         if args.engine != 1:

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <stdexcept>
+#include <vector>
 
 #include "bvh_device.h"
 #include "render_session.h"
@@ -751,6 +752,155 @@ void instanceBoxesDevice(const DevInstanceSrc* src, int n, float4* lo, float4* h
                          cudaStream_t st) {
   instanceBoxes<<<n, kBuildThreads, 0, st>>>(src, n, lo, hi, cent);
   cudaCheck(cudaGetLastError(), "instance boxes");
+}
+
+// ---- 4-wide collapse ------------------------------------------------------
+
+namespace {
+
+struct Collapse4Item {
+  int bin;  // binary node
+  int q;    // its 4-wide node
+};
+
+struct Collapse4Ctx {
+  const BvhNode* bin;
+  int numBin;
+  Bvh4Node* out;
+  int* qCount;     // 4-wide nodes allocated
+  int* nextCount;  // items of the next level
+  int* error;      // a link outside the binary array, or capacity exceeded
+  int qCap;
+};
+
+// Child `side` of a binary node: its box and link.
+__device__ __forceinline__ void binChild(const BvhNode& n, int side, float3& lo, float3& hi,
+                                         int& link) {
+  if (side == 0) {
+    lo = make_float3(n.xy0.x, n.xy0.z, n.zz.x);
+    hi = make_float3(n.xy0.y, n.xy0.w, n.zz.y);
+    link = n.link.x;
+  } else {
+    lo = make_float3(n.xy1.x, n.xy1.z, n.zz.z);
+    hi = make_float3(n.xy1.y, n.xy1.w, n.zz.w);
+    link = n.link.y;
+  }
+}
+
+__device__ __forceinline__ void setSlot(Bvh4Node& q, int k, float3 lo, float3 hi, int link) {
+  float4& xy = k == 0 ? q.xy0 : k == 1 ? q.xy1 : k == 2 ? q.xy2 : q.xy3;
+  float4& zz = k < 2 ? q.zz01 : q.zz23;
+  xy = make_float4(lo.x, hi.x, lo.y, hi.y);
+  if (k & 1) {
+    zz.z = lo.z;
+    zz.w = hi.z;
+  } else {
+    zz.x = lo.z;
+    zz.y = hi.z;
+  }
+  reinterpret_cast<int*>(&q.link)[k] = link;
+}
+
+// One thread per 4-wide node of the level: the binary node's children, each
+// leaf child kept as it is and each inner child replaced by its own two
+// children; inner grandchildren get 4-wide nodes of their own (next level).
+__global__ void collapse4Level(Collapse4Ctx c, const Collapse4Item* in, int nIn,
+                               Collapse4Item* next) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nIn) return;
+  const Collapse4Item it = in[i];
+  const BvhNode n = c.bin[it.bin];
+  Bvh4Node q;
+  const float3 far = make_float3(3e30f, 3e30f, 3e30f);
+  for (int k = 0; k < 4; k++) setSlot(q, k, far, far, ~0);
+  q.pad = make_int4(0, 0, 0, 0);
+  int k = 0;
+  for (int side = 0; side < 2; side++) {
+    float3 lo, hi;
+    int link;
+    binChild(n, side, lo, hi, link);
+    if (link < 0) {
+      setSlot(q, k++, lo, hi, link);
+      continue;
+    }
+    if (link >= c.numBin) {
+      atomicExch(c.error, 1);
+      return;
+    }
+    const BvhNode m = c.bin[link];
+    for (int s2 = 0; s2 < 2; s2++) {
+      float3 glo, ghi;
+      int g;
+      binChild(m, s2, glo, ghi, g);
+      if (g >= 0) {
+        if (g >= c.numBin) {
+          atomicExch(c.error, 1);
+          return;
+        }
+        const int qi = atomicAdd(c.qCount, 1);
+        if (qi >= c.qCap) {
+          atomicExch(c.error, 1);
+          return;
+        }
+        next[atomicAdd(c.nextCount, 1)] = Collapse4Item{g, qi};
+        g = qi;
+      }
+      setSlot(q, k++, glo, ghi, g);
+    }
+  }
+  c.out[it.q] = q;
+}
+
+}  // namespace
+
+int collapseBvh4Device(const BvhNode* bin, int numBin, const int* roots, int numRoots,
+                       Bvh4Node* out, int* outRoots, cudaStream_t st) {
+  if (numRoots < 1 || numRoots > numBin)
+    throw std::runtime_error("4-wide collapse: bad root count");
+  DevBuf items0, items1, counters;
+  items0.alloc((size_t)numBin * sizeof(Collapse4Item));
+  items1.alloc((size_t)numBin * sizeof(Collapse4Item));
+  counters.alloc(4 * sizeof(int));
+  std::vector<Collapse4Item> first(numRoots);
+  for (int r = 0; r < numRoots; r++) {
+    if (roots[r] < 0 || roots[r] >= numBin)
+      throw std::runtime_error("4-wide collapse: root outside the node array");
+    first[r] = Collapse4Item{roots[r], r};
+    outRoots[r] = r;
+  }
+  cudaCheck(cudaMemcpyAsync(items0.ptr, first.data(), first.size() * sizeof(Collapse4Item),
+                            cudaMemcpyHostToDevice, st),
+            "4-wide collapse roots");
+  int* cnt = (int*)counters.ptr;  // [0] nodes, [1] next items, [2] error
+  int init[4] = {numRoots, 0, 0, 0};
+  cudaCheck(cudaMemcpyAsync(cnt, init, sizeof init, cudaMemcpyHostToDevice, st),
+            "4-wide collapse counters");
+  Collapse4Ctx c;
+  c.bin = bin;
+  c.numBin = numBin;
+  c.out = out;
+  c.qCount = cnt;
+  c.nextCount = cnt + 1;
+  c.error = cnt + 2;
+  c.qCap = numBin;
+  int host[4] = {0, 0, 0, 0};
+  int nIn = numRoots;
+  void* in = items0.ptr;
+  void* nx = items1.ptr;
+  for (int level = 0; nIn > 0; level++) {
+    if (level > 4096) throw std::runtime_error("4-wide collapse: no progress");
+    cudaCheck(cudaMemsetAsync(cnt + 1, 0, sizeof(int), st), "4-wide collapse counters");
+    collapse4Level<<<(nIn + 127) / 128, 128, 0, st>>>(c, (const Collapse4Item*)in, nIn,
+                                                      (Collapse4Item*)nx);
+    cudaCheck(cudaGetLastError(), "4-wide collapse level");
+    cudaCheck(cudaMemcpyAsync(host, cnt, sizeof host, cudaMemcpyDeviceToHost, st),
+              "4-wide collapse count");
+    cudaCheck(cudaStreamSynchronize(st), "4-wide collapse level");
+    if (host[2]) throw std::runtime_error("4-wide collapse: malformed tree or capacity exceeded");
+    nIn = host[1];
+    std::swap(in, nx);
+  }
+  return host[0];
 }
 
 }  // namespace sdb

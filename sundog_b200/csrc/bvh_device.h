@@ -20,6 +20,15 @@ DevBvhStats buildBvhDevice(const float4* lo, const float4* hi, const float4* cen
                            int maxLeaf, int nodeBase, int primBase, BvhNode* nodes, int nodeCap,
                            int* order, cudaStream_t st);
 
+// 4-wide nodes from a binary node array (device, numBin nodes, links within
+// it): each 4-wide node holds the grandchildren of one binary node (a leaf
+// child kept as it is). roots (host, numRoots binary indices: the TLAS root,
+// then each BLAS root) map to outRoots (host), roots[r] -> r. out (device)
+// needs numBin entries. Returns the number of 4-wide nodes. Waits for the
+// stream once per level.
+int collapseBvh4Device(const BvhNode* bin, int numBin, const int* roots, int numRoots,
+                       Bvh4Node* out, int* outRoots, cudaStream_t st);
+
 // Object-space triangle boxes and centroids of a mesh.
 void meshBoxesDevice(const float3* pos, const uint3* idx, int n, float4* lo, float4* hi,
                      float4* cent, cudaStream_t st);

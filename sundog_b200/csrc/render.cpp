@@ -361,8 +361,16 @@ void DeviceScene::build(const SceneDesc& desc) {
   // A traversal keeps at most one stack entry per tree level (plus its
   // BLAS-entry entries), so trees this deep could fill the stack; reject them
   // rather than let a ray skip part of the scene.
+  if (SDB_BVH4 && !wide) {
+    // Three entries per 4-wide level (two binary levels) plus the marker.
+    const int need = 3 * ((tlasDepth + 2) / 2 + (blasDepth + 2) / 2) + 1;
+    if (need > kTraversal4Stack)
+      throw std::runtime_error("scene: BVH too deep for the 4-wide traversal stack (TLAS depth " +
+                               std::to_string(tlasDepth) + ", BLAS depth " +
+                               std::to_string(blasDepth) + ")");
+  }
   const int depthRoom = wide ? kCwTraversalStack - 4 : kTraversalStack - 2;
-  if (tlasDepth + blasDepth > depthRoom)
+  if (!(SDB_BVH4 && !wide) && tlasDepth + blasDepth > depthRoom)
     throw std::runtime_error("scene: BVH too deep for the traversal stack (TLAS depth " +
                              std::to_string(tlasDepth) + " + BLAS depth " +
                              std::to_string(blasDepth) + " > " + std::to_string(depthRoom) + ")");
@@ -390,6 +398,17 @@ void DeviceScene::build(const SceneDesc& desc) {
     else
       dNodes.upload(binNodes.data(), binNodes.size() * sizeof(BvhNode));
     dTris.upload(allTris.data(), allTris.size() * sizeof(float4));
+  }
+  if (SDB_BVH4 && !wide && numNodes > 0) {
+    // The 4-wide layout, collapsed on the device from the binary nodes; the
+    // TLAS root stays node 0 and each BLAS root moves to its 4-wide node.
+    std::vector<int> roots(1 + meshDescs.size()), roots4(roots.size());
+    roots[0] = 0;
+    for (size_t i = 0; i < meshDescs.size(); i++) roots[1 + i] = meshDescs[i].root;
+    dNodes4.alloc(numNodes * sizeof(Bvh4Node));
+    collapseBvh4Device((const BvhNode*)dNodes.ptr, (int)numNodes, roots.data(), (int)roots.size(),
+                       (Bvh4Node*)dNodes4.ptr, roots4.data(), 0);
+    for (size_t i = 0; i < meshDescs.size(); i++) meshDescs[i].root = roots4[1 + i];
   }
   dInst.upload(inst.data(), inst.size() * sizeof(SdInstance));
   dMeshes.upload(meshDescs.data(), meshDescs.size() * sizeof(SdMesh));
@@ -578,6 +597,7 @@ void DeviceScene::fillLaunch(SdLaunch& l) const {
   l.flames = (const SdFlame*)dFlames.ptr;
   l.numFlames = (int)scene.flames.size();
   l.nodes = wideNodes ? nullptr : (const BvhNode*)dNodes.ptr;
+  l.nodes4 = (const Bvh4Node*)dNodes4.ptr;
   l.cw = wideNodes ? (const CwNode*)dNodes.ptr : nullptr;
   l.tris = (const float4*)dTris.ptr;
   l.inst = (const SdInstance*)dInst.ptr;

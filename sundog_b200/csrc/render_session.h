@@ -83,6 +83,7 @@ struct DeviceScene {
   std::vector<MeshBufs> meshBufs;
   std::vector<DevBuf> lightBufs;
   DevBuf dNodes, dTris, dInst, dMeshes, dTex, dMat, dLights, dFlames;
+  DevBuf dNodes4;  // the 4-wide layout (SDB_BVH4), collapsed from dNodes
   std::vector<SdLight> lights;  // host copy of the device light list
 
   void build(const SceneDesc& desc);

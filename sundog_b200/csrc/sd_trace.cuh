@@ -28,7 +28,8 @@
 
 namespace sdb {
 
-constexpr int kStackSize = kTraversalStack;
+// The 4-wide walk pushes up to three entries per level.
+constexpr int kStackSize = SDB_BVH4 ? kTraversal4Stack : kTraversalStack;
 constexpr int kPop = (int)0x80000000;        // "take the next stack entry"
 constexpr int kToTlas = (int)0x80000001;     // marker: leave the BLAS
 
@@ -150,6 +151,18 @@ __device__ __forceinline__ void boxPair(const BvhNode& nd, float3 oi, float3 id,
   hb = n1 <= f1;
   ta = n0;
   tb = n1;
+}
+
+// Orders (d, l) pairs: the smaller distance first, ties keep their order.
+__device__ __forceinline__ void cswap(float& da, int& la, float& db, int& lb) {
+  if (db < da) {
+    float td = da;
+    da = db;
+    db = td;
+    int tl = la;
+    la = lb;
+    lb = tl;
+  }
 }
 
 __device__ __forceinline__ float safeInv(float x) {
@@ -578,6 +591,50 @@ __device__ __forceinline__ int binTravStep(BinTrav& t, TravStack& stack, const S
                                            TraceCount* cnt) {
   const float tmin = 0.0f;
   if (COUNT) countWarp(cnt, cnt->travIters, cnt->travLanes);
+#if SDB_BVH4
+  if (t.cur >= 0) {
+    // Four child boxes; the nearest hit child next, the other hits pushed
+    // farthest first.
+    const float4* np = reinterpret_cast<const float4*>(lp.nodes4 + t.cur);
+    if (COUNT) cnt->boxTests += 4;
+    const float inf = __int_as_float(0x7f800000);
+    float d0, d1, d2, d3;
+    {
+      BvhNode pr;
+      pr.xy0 = __ldg(np);
+      pr.xy1 = __ldg(np + 1);
+      pr.zz = __ldg(np + 2);
+      bool h0, h1;
+      boxPair(pr, t.oi, t.id, tmin, t.tmax, d0, d1, h0, h1);
+      d0 = h0 ? d0 : inf;
+      d1 = h1 ? d1 : inf;
+    }
+    {
+      BvhNode pr;
+      pr.xy0 = __ldg(np + 3);
+      pr.xy1 = __ldg(np + 4);
+      pr.zz = __ldg(np + 5);
+      bool h2, h3;
+      boxPair(pr, t.oi, t.id, tmin, t.tmax, d2, d3, h2, h3);
+      d2 = h2 ? d2 : inf;
+      d3 = h3 ? d3 : inf;
+    }
+    const int4 lk = __ldg(reinterpret_cast<const int4*>(np + 6));
+    int l0 = lk.x, l1 = lk.y, l2 = lk.z, l3 = lk.w;
+    cswap(d0, l0, d1, l1);
+    cswap(d2, l2, d3, l3);
+    cswap(d0, l0, d2, l2);
+    cswap(d1, l1, d3, l3);
+    cswap(d1, l1, d2, l2);
+    if (!(d0 < inf)) return binTravPop(t, stack, sink);
+    // Always room: the scene build bounds the tree depths by the stack.
+    if (d3 < inf && t.sp < kStackSize) stack[t.sp++] = l3;
+    if (d2 < inf && t.sp < kStackSize) stack[t.sp++] = l2;
+    if (d1 < inf && t.sp < kStackSize) stack[t.sp++] = l1;
+    t.cur = l0;
+    return kTravMore;
+  }
+#endif
   if (t.cur >= 0) {
     BvhNode nd = loadNode(lp.nodes, t.cur);
     if (COUNT) cnt->boxTests += 2;

@@ -121,6 +121,29 @@ struct __align__(16) BvhNode {
   int4 link;    // child0, child1, cnt0, cnt1
 };
 
+// Node layout the traversal reads: 1 (default) the 4-wide nodes below,
+// collapsed from the binary build; 0 the binary nodes themselves (measured
+// on the bench frames, Mrays/s, 4-wide / binary: config 1 1,652 / 1,622,
+// config 0 2,772 / 2,747, config 2 2,491 / 2,424).
+#ifndef SDB_BVH4
+#define SDB_BVH4 1
+#endif
+
+// 4-wide node (128 bytes, seven 16-byte loads), collapsed from the binary
+// tree on the device (bvh_device.cu: each node holds the grandchildren of
+// one binary node, or its child where that child is a leaf): the boxes of
+// children 0-1 and of children 2-3 each in BvhNode's box layout (so a pair
+// is tested with the binary node's arithmetic while the other pair is not
+// yet loaded), then the four links (inner node index >= 0, leaf code < 0 as
+// in BvhNode). An unused slot has the far point (3e30, 3e30, 3e30) as its
+// box, which no ray reaches within its tmax.
+struct __align__(16) Bvh4Node {
+  float4 xy0, xy1, zz01;  // children 0 and 1: lo.x hi.x lo.y hi.y / ... / lo.z hi.z lo.z hi.z
+  float4 xy2, xy3, zz23;  // children 2 and 3
+  int4 link;
+  int4 pad;
+};
+
 // Compressed 8-wide node (80 bytes, five 16-byte loads), after Ylitie,
 // Karras and Laine, "Efficient Incoherent Ray Traversal on GPUs Through
 // Compressed Wide BVHs" (HPG 2017). Child boxes are stored as 8-bit offsets
@@ -145,6 +168,9 @@ constexpr int kCwLeafMax = 3;  // primitives per leaf slot
 // TLAS depth + BLAS depth + 4 <= kCwTraversalStack. The scene build rejects
 // deeper trees, so no traversal ever finds its stack full.
 constexpr int kTraversalStack = 64;
+// The 4-wide walk (SDB_BVH4) pushes at most three entries per 4-wide level
+// (two binary levels) plus one marker at a BLAS entry.
+constexpr int kTraversal4Stack = 96;
 constexpr int kCwTraversalStack = 48;
 
 // Visit counts of the traversal, gathered only by the counting variant of the
@@ -205,6 +231,7 @@ struct SdLaunch {
   int numFlames;
 
   const BvhNode* nodes;
+  const Bvh4Node* nodes4;  // 4-wide nodes (the SDB_BVH4 layout), TLAS root first
   const CwNode* cw;       // 8-wide nodes (TLAS root first, then each BLAS)
   const float4* tris;     // 3 float4 per leaf-ordered triangle; .w of the
                           // first holds the mesh-local triangle index
