@@ -152,6 +152,29 @@ __global__ void __launch_bounds__(kRenderBlock) wfStart() {
     refill<GUIDE>(slot, 0);
 }
 
+// Camera paths into the pool without atomics, for frames whose 8x8 pixel
+// tiles cover the image exactly (every path id is a pixel sample, so
+// refill's id counter and list appends would only number the slots in
+// order): slot i takes path i, the live list is the identity, and the list
+// length and path counter continue from n = min(pool, paths). The same
+// paths in the same slots as wfStart.
+template <int GUIDE>
+__global__ void __launch_bounds__(kRenderBlock) wfStartDirect(unsigned n) {
+  const WfPool& pool = c_pool;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    pool.counts[0] = n;
+    *c_wlp.pathCounter = n;
+  }
+  for (unsigned slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n;
+       slot += gridDim.x * blockDim.x) {
+    Path p;
+    startPath(c_wlp, slot, p);
+    pool.paths[slot].v = p;
+    if (GUIDE & kGuideRecord) pool.trails[slot].v.n = 0;
+    pool.lists[0][slot] = (int)slot;
+  }
+}
+
 // Stores a closest-hit candidate straight into the slot's hit record (three
 // 16-byte stores), so the trace loop keeps no hit fields in registers: each
 // closer hit overwrites the record, and a ray that hits nothing leaves the
@@ -714,7 +737,7 @@ static double evMs(cudaEvent_t a, cudaEvent_t b) {
 // iterations until no path is live (the launch block or batch is already in
 // constant memory). Returns the kernels launched.
 static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, int mode,
-                   bool shadowFetch, WfStageTimes* times = nullptr) {
+                   bool shadowFetch, bool directStart, WfStageTimes* times = nullptr) {
   const bool timed = times != nullptr;
   if (timed && !b.ev[0])
     for (cudaEvent_t& e : b.ev) cudaCheck(cudaEventCreate(&e), "stage timing events");
@@ -736,8 +759,13 @@ static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, i
   cudaCheck(cudaMemsetAsync(b.counts.ptr, 0, b.counts.bytes, st), "wavefront counts");
   int launches = 0;
   if (timed) cudaEventRecord(b.ev[0], st);
+  const unsigned direct = (unsigned)pool.cap;
   if (mode & kWfServe)
     wfStart<kWfServe><<<b.gridStart, kRenderBlock, 0, st>>>();
+  else if (directStart && (mode & kGuideRecord))
+    wfStartDirect<kGuideRecord><<<b.gridStart, kRenderBlock, 0, st>>>(direct);
+  else if (directStart)
+    wfStartDirect<0><<<b.gridStart, kRenderBlock, 0, st>>>(direct);
   else if (mode & kGuideRecord)
     wfStart<kGuideRecord><<<b.gridStart, kRenderBlock, 0, st>>>();
   else
@@ -795,7 +823,9 @@ int wfRender(const SdLaunch& lp, WfBuffers& b, cudaStream_t st, int guide, WfSta
   if (guide & kGuideRecord) b.ensureTrails();
   cudaCheck(cudaMemcpyToSymbolAsync(c_wlp, &lp, sizeof lp, 0, cudaMemcpyHostToDevice, st),
             "wavefront launch block");
-  return runPool(b, st, lp.numPaths, guide, lp.numInstances >= kShadowFetchInstances, times);
+  const bool exactTiles = lp.shardCount <= 1 && lp.npixPad == lp.width * lp.height;
+  return runPool(b, st, lp.numPaths, guide, lp.numInstances >= kShadowFetchInstances, exactTiles,
+                 times);
 }
 
 cudaError_t wfSetJobs(const SdLaunch* table, cudaStream_t st) {
@@ -806,7 +836,7 @@ cudaError_t wfSetJobs(const SdLaunch* table, cudaStream_t st) {
 int wfRenderBatch(const ServeBatch& batch, WfBuffers& b, cudaStream_t st, int maxInstances) {
   cudaCheck(cudaMemcpyToSymbolAsync(c_wbatch, &batch, sizeof batch, 0, cudaMemcpyHostToDevice, st),
             "wavefront batch");
-  return runPool(b, st, batch.numPaths, kWfServe, maxInstances >= kShadowFetchInstances);
+  return runPool(b, st, batch.numPaths, kWfServe, maxInstances >= kShadowFetchInstances, false);
 }
 
 }  // namespace sdb
