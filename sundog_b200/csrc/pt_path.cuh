@@ -109,8 +109,15 @@ __device__ __forceinline__ bool startPath(const SdLaunch& lp, unsigned long long
     px = (tile % lp.shardTilesX) * 64 + (block & 7) * 8 + (within & 7);
     py = (tile / lp.shardTilesX) * 64 + (block >> 3) * 8 + (within >> 3);
   } else {
-    sLocal = (int)(id / (unsigned long long)lp.npixPad);
-    int rem = (int)(id - (unsigned long long)sLocal * lp.npixPad);
+    int rem;
+    if (id < (1ull << 32)) {  // a 32-bit division: the common case, far cheaper
+      const unsigned id32 = (unsigned)id;
+      sLocal = (int)(id32 / (unsigned)lp.npixPad);
+      rem = (int)(id32 - (unsigned)sLocal * (unsigned)lp.npixPad);
+    } else {
+      sLocal = (int)(id / (unsigned long long)lp.npixPad);
+      rem = (int)(id - (unsigned long long)sLocal * lp.npixPad);
+    }
     int tile = rem >> 6, within = rem & 63;
     int tx = tile % lp.tilesX, ty = tile / lp.tilesX;
     px = tx * 8 + (within & 7);

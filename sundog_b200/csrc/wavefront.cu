@@ -57,12 +57,12 @@ __device__ __forceinline__ const SdLaunch& slotLaunch(int slot) {
 #ifndef SDB_WF_TRACE_BLOCKS
 #define SDB_WF_TRACE_BLOCKS 8
 #endif
-// Resident blocks per SM the stage kernels are compiled for (measured on the
-// instancing frame with a 64 M-slot pool: traversal 8 -> 64 registers,
-// shading 5 -> 102 registers, 1,136 Mrays/s against 1,115 at 4 shading
-// blocks; 877 / 835 / 842 at 6 / 10 / 12 traversal blocks with 4 M slots).
+// Resident blocks per SM the stage kernels are compiled for: traversal 8 ->
+// 64 registers, shading 6 -> 80 registers (config 1 / config 2, Mrays/s:
+// 1,716 / 2,558 at 6 shading blocks, 1,697 / 2,507 at 5 (102 registers),
+// 1,648 / 2,402 at 4).
 #ifndef SDB_WF_SHADE_BLOCKS
-#define SDB_WF_SHADE_BLOCKS 5
+#define SDB_WF_SHADE_BLOCKS 6
 #endif
 
 // Slot index for an append to a list by the calling lanes together.
