@@ -129,7 +129,14 @@ SDB_HD void flameAt(const SdFlame& fl, float3 p, float& sigma, float3& eps) {
   if (h <= 0.0f || h >= 1.0f) return;
   float rx = p.x - fl.base.x, rz = p.z - fl.base.z;
   float d = sqrtf(rx * rx + rz * rz) / fl.radius;
-  float prof = 3.2f * sqrtf(h) * powf(1.0f - h, 1.55f);
+  const float sh = sqrtf(h);
+  // (1 - h)^1.55 <= 1 - h on [0, 1], so 3.2001 sqrt(h) (1 - h) bounds the
+  // profile from above (the margin covers powf's error and the roundings);
+  // where even that bound puts the step outside the mask for every noise
+  // value (the test below with 1.4502 for 1.45), the exact test would too:
+  // the empty medium, without powf.
+  if (d >= 1.4502f * fmaxf(3.2001f * sh * (1.0f - h), 1e-3f)) return;
+  float prof = 3.2f * sh * powf(1.0f - h, 1.55f);
   const float dp = d / fmaxf(prof, 1e-3f);
   // The noise term n - 0.45 is at least -0.45 (fBm is non-negative), so where
   // dp - 0.45 already reaches the mask's outer edge (1) the mask is 0 for
