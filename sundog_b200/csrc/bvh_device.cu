@@ -703,8 +703,7 @@ DevBvhStats buildBvhDevice(const float4* lo, const float4* hi, const float4* cen
   c.primBase = primBase;
   c.nodeCap = nodeCap;
   c.rangeCap = n;
-  int* pinned = nullptr;
-  cudaCheck(cudaMallocHost((void**)&pinned, 4 * sizeof(int)), "device BVH pinned");
+  int* pinned = reinterpret_cast<int*>(pinnedWords());
   try {
     int nIn = 1;
     void* idsIn = ids0.ptr;
@@ -729,10 +728,10 @@ DevBvhStats buildBvhDevice(const float4* lo, const float4* hi, const float4* cen
     stats.nodes = pinned[0];
     stats.maxDepth = pinned[1];
   } catch (...) {
-    cudaFreeHost(pinned);
+    returnPinnedWords(reinterpret_cast<unsigned*>(pinned));
     throw;
   }
-  cudaFreeHost(pinned);
+  returnPinnedWords(reinterpret_cast<unsigned*>(pinned));
   return stats;
 }
 

@@ -46,6 +46,29 @@ void cudaCheck(cudaError_t e, const char* what) {
     throw std::runtime_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
 }
 
+static std::mutex g_pinnedMu;
+static std::vector<unsigned*> g_pinnedFree;
+
+unsigned* pinnedWords() {
+  {
+    std::lock_guard<std::mutex> lock(g_pinnedMu);
+    if (!g_pinnedFree.empty()) {
+      unsigned* p = g_pinnedFree.back();
+      g_pinnedFree.pop_back();
+      return p;
+    }
+  }
+  unsigned* p = nullptr;
+  cudaCheck(cudaMallocHost((void**)&p, 4 * sizeof(unsigned)), "pinned words");
+  return p;
+}
+
+void returnPinnedWords(unsigned* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lock(g_pinnedMu);
+  g_pinnedFree.push_back(p);
+}
+
 void DevBuf::alloc(size_t n) {
   release();
   if (n == 0) return;

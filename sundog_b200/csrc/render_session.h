@@ -27,6 +27,12 @@ struct WfStageTimes {
 };
 
 
+// Four pinned host words for a counter read-back, from a process-wide free
+// list (a pinned allocation costs more than the render of a small frame);
+// returned words are kept for the next caller, never freed.
+unsigned* pinnedWords();
+void returnPinnedWords(unsigned* p);
+
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;

@@ -27,6 +27,7 @@
 #include <memory>
 #include <mutex>
 #include <stdexcept>
+#include <vector>
 
 #include "pt_path.cuh"
 #include "serve.h"
@@ -636,17 +637,21 @@ void WfBuffers::ensure(int slots) {
   const size_t fit = std::max<size_t>(budget / wfSlotBytes(), (size_t)1 << 20);
   slots = (int)std::min<size_t>((size_t)slots, fit);
   if (slots <= cap) return;
-  paths.alloc((size_t)slots * sizeof(PoolSlot<Path>));
-  verts.alloc((size_t)slots * sizeof(PoolSlot<Vertex>));
-  hits.alloc((size_t)slots * sizeof(PoolSlot<TraceHit>));
-  trs.alloc((size_t)slots * sizeof(float4));
-  pending.alloc((size_t)slots);
-  list0.alloc((size_t)slots * sizeof(int));
-  list1.alloc((size_t)slots * sizeof(int));
-  shadow.alloc((size_t)slots * sizeof(int));
-  jobs.alloc((size_t)slots);
+  const size_t n = (size_t)slots;
+  const size_t sizes[9] = {n * sizeof(PoolSlot<Path>), n * sizeof(PoolSlot<Vertex>),
+                           n * sizeof(PoolSlot<TraceHit>), n * sizeof(float4), n,
+                           n * sizeof(int), n * sizeof(int), n * sizeof(int), n};
+  size_t offs[9], total = 0;
+  for (int k = 0; k < 9; k++) {
+    offs[k] = total;
+    total += (sizes[k] + 255) & ~(size_t)255;
+  }
+  slab.release();
+  slab.alloc(total);
+  void** parts[9] = {&paths, &verts, &hits, &trs, &pending, &list0, &list1, &shadow, &jobs};
+  for (int k = 0; k < 9; k++) *parts[k] = (char*)slab.ptr + offs[k];
   if (!counts.ptr) counts.alloc(8 * sizeof(unsigned));
-  if (!hostCount) cudaCheck(cudaMallocHost((void**)&hostCount, 4 * sizeof(unsigned)), "pinned count");
+  if (!hostCount) hostCount = pinnedWords();
   cap = slots;
   gridTrace = gridFor(wfTraceFetch<false>);
   gridShadeA = gridFor(wfShadeA<0>);
@@ -662,7 +667,7 @@ void WfBuffers::ensureTrails() {
 }
 
 WfBuffers::~WfBuffers() {
-  if (hostCount) cudaFreeHost(hostCount);
+  if (hostCount) returnPinnedWords(hostCount);
   for (cudaEvent_t& e : ev)
     if (e) cudaEventDestroy(e);
 }
@@ -742,17 +747,17 @@ static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, i
   if (timed && !b.ev[0])
     for (cudaEvent_t& e : b.ev) cudaCheck(cudaEventCreate(&e), "stage timing events");
   WfPool pool;
-  pool.paths = (PoolSlot<Path>*)b.paths.ptr;
-  pool.verts = (PoolSlot<Vertex>*)b.verts.ptr;
-  pool.hits = (PoolSlot<TraceHit>*)b.hits.ptr;
-  pool.trs = (float4*)b.trs.ptr;
-  pool.pending = (unsigned char*)b.pending.ptr;
-  pool.lists[0] = (int*)b.list0.ptr;
-  pool.lists[1] = (int*)b.list1.ptr;
-  pool.shadowList = (int*)b.shadow.ptr;
+  pool.paths = (PoolSlot<Path>*)b.paths;
+  pool.verts = (PoolSlot<Vertex>*)b.verts;
+  pool.hits = (PoolSlot<TraceHit>*)b.hits;
+  pool.trs = (float4*)b.trs;
+  pool.pending = (unsigned char*)b.pending;
+  pool.lists[0] = (int*)b.list0;
+  pool.lists[1] = (int*)b.list1;
+  pool.shadowList = (int*)b.shadow;
   pool.counts = (unsigned*)b.counts.ptr;
   pool.trails = (PoolSlot<GuideTrail>*)b.trails.ptr;
-  pool.jobs = (unsigned char*)b.jobs.ptr;
+  pool.jobs = (unsigned char*)b.jobs;
   pool.cap = (int)std::min<unsigned long long>((unsigned long long)b.cap, numPaths);
   cudaCheck(cudaMemcpyToSymbolAsync(c_pool, &pool, sizeof pool, 0, cudaMemcpyHostToDevice, st),
             "wavefront pool");

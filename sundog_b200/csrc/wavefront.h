@@ -43,9 +43,13 @@ struct WfPool {
 
 // Host-owned pool storage, grown on demand.
 struct WfBuffers {
-  DevBuf paths, verts, hits, trs, pending, list0, list1, shadow, counts, jobs;
+  // One device allocation holds every per-slot array (carved at 256-byte
+  // boundaries), so a pool costs one cudaMalloc and one cudaFree.
+  DevBuf slab, counts;
+  void *paths = nullptr, *verts = nullptr, *hits = nullptr, *trs = nullptr, *pending = nullptr,
+       *list0 = nullptr, *list1 = nullptr, *shadow = nullptr, *jobs = nullptr;
   DevBuf trails;  // allocated by the first training-record pass
-  unsigned* hostCount = nullptr;   // pinned: the four list counters
+  unsigned* hostCount = nullptr;   // pinned: the four list counters (from a process-wide free list)
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // stage timing
   int cap = 0;
   int trailCap = 0;
