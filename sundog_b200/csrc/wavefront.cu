@@ -59,11 +59,14 @@ __device__ __forceinline__ const SdLaunch& slotLaunch(int slot) {
 #define SDB_WF_TRACE_BLOCKS 8
 #endif
 // Resident blocks per SM the stage kernels are compiled for: traversal 8 ->
-// 64 registers, shading 6 -> 80 registers (config 1 / config 2, Mrays/s:
-// 1,716 / 2,558 at 6 shading blocks, 1,697 / 2,507 at 5 (102 registers),
-// 1,648 / 2,402 at 4).
+// 64 registers, shading 5 -> 102 registers. Shading at 6 blocks (80
+// registers) gains on config 1 and 2 (1,716 / 2,558 against 1,697 / 2,507
+// Mrays/s) and loses on config 0 and the gallery scenes, whose shading
+// spills more at 80 registers (01-marble-run 4,476 against 4,709,
+// 02-cornell-lume 3,673 against 3,819); 4 blocks lose on all (1,648 /
+// 2,402 on configs 1 / 2).
 #ifndef SDB_WF_SHADE_BLOCKS
-#define SDB_WF_SHADE_BLOCKS 6
+#define SDB_WF_SHADE_BLOCKS 5
 #endif
 
 // Slot index for an append to a list by the calling lanes together.

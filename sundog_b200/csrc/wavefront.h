@@ -95,6 +95,9 @@ int wfRenderBatch(const ServeBatch& batch, WfBuffers& b, cudaStream_t st, int ma
 
 // Scenes with at least this many instances trace their shadow rays with
 // dynamic fetch (wfShadowFetch), smaller ones one ray per thread (wfShadow).
-constexpr int kShadowFetchInstances = 64;
+#ifndef SDB_SHADOW_FETCH_INSTANCES
+#define SDB_SHADOW_FETCH_INSTANCES 64
+#endif
+constexpr int kShadowFetchInstances = SDB_SHADOW_FETCH_INSTANCES;
 
 }  // namespace sdb
