@@ -21,10 +21,12 @@
 // for bit. sin(theta) comes from the host (sinf, as in the reference) per row.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <stdexcept>
 
 #include "cdf_build.h"
 #include "render_session.h"
+#include "sd_lights.cuh"
 
 namespace sdb {
 
@@ -165,6 +167,25 @@ __global__ void __launch_bounds__(kScanThreads) meshLightCdf(const float3* __res
     if (threadIdx.x == 0) cdf[n] = 1.0f;
   }
   if (threadIdx.x == 0) *total = t;
+}
+
+// Guide entries of `rows` CDFs of n entries (row r at cdf + r * stride):
+// entry k of a row is the index the plain search (sd_lights.cuh cdfSearch)
+// returns for u = k / kCdfGuide, exact in FP32.
+__global__ void cdfGuide(const float* cdf, int n, size_t stride, int rows, int* guide) {
+  const int total = rows * (kCdfGuide + 1);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const int r = i / (kCdfGuide + 1), k = i - r * (kCdfGuide + 1);
+    guide[i] = cdfSearch(cdf + (size_t)r * stride, n, (float)k / (float)kCdfGuide);
+  }
+}
+
+void buildCdfGuideDevice(const float* cdf, int n, size_t stride, int rows, int* guide,
+                         cudaStream_t st) {
+  const int total = rows * (kCdfGuide + 1);
+  const int grid = std::max(1, std::min((total + 255) / 256, 148 * 8));
+  cdfGuide<<<grid, 256, 0, st>>>(cdf, n, stride, rows, guide);
+  cudaCheck(cudaGetLastError(), "CDF guide launch");
 }
 
 void buildEnvCdfDevice(const float4* texels, int w, int h, float* marg, float* cond,

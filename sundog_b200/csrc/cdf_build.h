@@ -14,6 +14,12 @@ namespace sdb {
 void buildEnvCdfDevice(const float4* texels, int w, int h, float* marg, float* cond,
                        bool& degenerate, cudaStream_t st);
 
+// Search guides (sd_types.h kCdfGuide) of `rows` CDFs of n entries each,
+// row r at cdf + r * stride (device); guide receives rows x (kCdfGuide + 1)
+// ints (device). Does not wait for the stream.
+void buildCdfGuideDevice(const float* cdf, int n, size_t stride, int rows, int* guide,
+                         cudaStream_t st);
+
 // World-space vertices (worldPos, numVerts) and area CDF (cdf, numTris + 1
 // floats) of a mesh instance whose object-space vertices and indices are on
 // the device; returns the total area (FP64). Waits for the stream.

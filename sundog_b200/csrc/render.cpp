@@ -242,9 +242,17 @@ void DeviceScene::build(const SceneDesc& desc) {
     if (degenerate && scene.env.importance)
       std::fprintf(stderr, "envmap: %s has zero luminance, falling back to uniform sampling\n",
                    scene.env.file.c_str());
+    // Search guides: the marginal's, then each row's conditional's.
+    envGuide.alloc((size_t)(envH + 1) * (kCdfGuide + 1) * sizeof(int));
+    int* guide = (int*)envGuide.ptr;
+    buildCdfGuideDevice((const float*)envMarg.ptr, envH + 1, 0, 1, guide, 0);
+    buildCdfGuideDevice((const float*)envCond.ptr, envW + 1, (size_t)envW + 1, envH,
+                        guide + (kCdfGuide + 1), 0);
     env.texels = (const float4*)envTex.ptr;
     env.margCdf = (const float*)envMarg.ptr;
     env.condCdf = (const float*)envCond.ptr;
+    env.margGuide = guide;
+    env.condGuide = guide + (kCdfGuide + 1);
     env.width = envW;
     env.height = envH;
     env.rotate = scene.env.rotateDeg * kPi / 180.0f;

@@ -84,7 +84,7 @@ struct DeviceScene {
   size_t meshTriangles = 0, numNodes = 0, numTris = 0, deviceBytes = 0;
   int tlasDepth = 0, blasDepth = 0;
   double loadMs = 0, buildMs = 0;
-  DevBuf envTex, envMarg, envCond;
+  DevBuf envTex, envMarg, envCond, envGuide;  // envGuide: marginal, then each row's
   std::vector<DevBuf> texImages;
   std::vector<MeshBufs> meshBufs;
   std::vector<DevBuf> lightBufs;

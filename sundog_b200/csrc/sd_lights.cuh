@@ -22,8 +22,7 @@ struct LightDraw {
 
 // Largest i in [0, n-2] with cdf[i] <= u. (device/env_light.cuh:36-43;
 // the mesh-light search in device/light_sample.cuh:99-103 is the same.)
-SDB_HD int cdfSearch(const float* cdf, int n, float u) {
-  int lo = 0, hi = n - 1;
+SDB_HD int cdfSearchIn(const float* cdf, int lo, int hi, float u) {
   while (lo + 1 < hi) {
     int mid = (lo + hi) >> 1;
     if (cdf[mid] <= u)
@@ -32,6 +31,20 @@ SDB_HD int cdfSearch(const float* cdf, int n, float u) {
       hi = mid;
   }
   return lo;
+}
+
+SDB_HD int cdfSearch(const float* cdf, int n, float u) { return cdfSearchIn(cdf, 0, n - 1, u); }
+
+// The same index through the CDF's guide (kCdfGuide + 1 entries; null: the
+// plain search). For a non-decreasing CDF the search returns the last index
+// i <= n - 2 with cdf[i] <= u, a non-decreasing function of u, so for u in
+// [k / K, (k + 1) / K) (exact bounds: K is a power of two) it lies between
+// guide[k] and guide[k + 1], and cdf[guide[k]] <= u < cdf[guide[k + 1] + 1]
+// (or guide[k + 1] = n - 2) keep the loop's invariants.
+SDB_HD int cdfSearchGuided(const float* cdf, int n, const int* guide, float u) {
+  if (!guide) return cdfSearch(cdf, n, u);
+  const int k = min(max((int)(u * (float)kCdfGuide), 0), kCdfGuide - 1);
+  return cdfSearchIn(cdf, guide[k], min(guide[k + 1] + 1, n - 1), u);
 }
 
 // ---- environment ------------------------------------------------------------
@@ -70,12 +83,14 @@ SDB_HD LightDraw envDraw(const SdEnv& e, Pcg& rng) {
     s.ok = true;
     return s;
   }
-  int row = cdfSearch(e.margCdf, e.height + 1, rn.x);
+  int row = cdfSearchGuided(e.margCdf, e.height + 1, e.margGuide, rn.x);
   float dm = e.margCdf[row + 1] - e.margCdf[row];
   float dv = dm > 0.0f ? (rn.x - e.margCdf[row]) / dm : 0.5f;
   float v = (row + dv) / e.height;
   const float* cdf = e.condCdf + (size_t)row * (e.width + 1);
-  int col = cdfSearch(cdf, e.width + 1, rn.y);
+  int col = cdfSearchGuided(cdf, e.width + 1,
+                            e.condGuide ? e.condGuide + (size_t)row * (kCdfGuide + 1) : nullptr,
+                            rn.y);
   float dc = cdf[col + 1] - cdf[col];
   float du = dc > 0.0f ? (rn.y - cdf[col]) / dc : 0.5f;
   float u = (col + du) / e.width;

@@ -65,10 +65,17 @@ struct SdLight {
   float mNgSign;
 };
 
+// Guide of a CDF search: kCdfGuide + 1 ints per CDF, entry k the index the
+// search returns for u = k / kCdfGuide (cdf_build.cu), so a search for u
+// starts from the bracket of its bucket.
+constexpr int kCdfGuide = 256;
+
 struct SdEnv {
   const float4* texels;  // width x height, row 0 = zenith
   const float* margCdf;  // height + 1
   const float* condCdf;  // height x (width + 1)
+  const int* margGuide;  // kCdfGuide + 1
+  const int* condGuide;  // height x (kCdfGuide + 1)
   int width, height;
   float rotate;          // radians about +Y
   float intensity;

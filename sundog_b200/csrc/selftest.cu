@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/sundog_api.h"
+#include "cdf_build.h"
 #include "abi_util.h"
 #include "bvh_build.h"
 #include "render_session.h"
@@ -44,9 +45,11 @@ struct StNoiseIn { float3 p; unsigned seed; float3 ns, wo; float amp, freq; };
 struct StNoiseOut { float fbm, vnoise; float3 wave; };
 // 9: CDF search. in {u}; shared cdf passed as a second block; out {index}
 // 10: bilinear filter of a float4 grid. in {u, v}; out {rgba}
+// 11: CDF search through the CDF's guide (built on the device from the
+//     shared cdf, as for the environment's tables). in {u}; out {index}
 
 __global__ void stKernel(int which, const void* in, int n, void* out, const float* aux, int auxN,
-                         int auxW, int auxH) {
+                         int auxW, int auxH, const int* guide) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   switch (which) {
@@ -158,6 +161,11 @@ __global__ void stKernel(int which, const void* in, int n, void* out, const floa
       ((float4*)out)[i] = sampleFloat4((const float4*)aux, auxW, auxH, uv.x, uv.y);
       break;
     }
+    case 11: {
+      float u = ((const float*)in)[i];
+      ((int*)out)[i] = cdfSearchGuided(aux, auxN, guide, u);
+      break;
+    }
   }
 }
 
@@ -173,6 +181,7 @@ static size_t itemIn(int which) {
     case 8: return sizeof(StNoiseIn);
     case 9: return sizeof(float);
     case 10: return sizeof(float2);
+    case 11: return sizeof(float);
   }
   return 0;
 }
@@ -188,6 +197,7 @@ static size_t itemOut(int which) {
     case 8: return sizeof(StNoiseOut);
     case 9: return sizeof(int);
     case 10: return sizeof(float4);
+    case 11: return sizeof(int);
   }
   return 0;
 }
@@ -206,22 +216,22 @@ extern "C" __attribute__((visibility("default"))) int sundog_selftest_sizes(int 
   return SUNDOG_OK;
 }
 
-// `in` holds n items; for which = 9 / 10 the auxiliary table (cdf floats, or
-// a W x H float4 grid) follows the items: int count (9) or int W, int H (10),
-// then the floats.
+// `in` holds n items; for which = 9 / 10 / 11 the auxiliary table (cdf
+// floats, or a W x H float4 grid) follows the items: int count (9, 11) or
+// int W, int H (10), then the floats.
 extern "C" int sundog_selftest(int which, const void* in, int n, void* out, size_t out_bytes) {
   SDB_TRY
   size_t ib = itemIn(which), ob = itemOut(which);
   if (!ib) throw std::runtime_error("selftest: unknown function id");
   if (n <= 0 || !in || !out) throw std::runtime_error("selftest: empty batch");
   if (out_bytes < ob * (size_t)n) throw std::runtime_error("selftest: output buffer too small");
-  DevBuf din, dout, daux;
+  DevBuf din, dout, daux, dguide;
   din.upload(in, ib * n);
   dout.alloc(ob * n);
   int auxN = 0, auxW = 0, auxH = 0;
-  if (which == 9 || which == 10) {
+  if (which == 9 || which == 10 || which == 11) {
     const char* tail = (const char*)in + ib * n;
-    if (which == 9) {
+    if (which == 9 || which == 11) {
       std::memcpy(&auxN, tail, sizeof(int));
       if (auxN < 2) throw std::runtime_error("selftest: cdf needs >= 2 entries");
       daux.upload(tail + sizeof(int), (size_t)auxN * sizeof(float));
@@ -232,8 +242,12 @@ extern "C" int sundog_selftest(int which, const void* in, int n, void* out, size
       daux.upload(tail + 2 * sizeof(int), (size_t)auxW * auxH * 4 * sizeof(float));
     }
   }
+  if (which == 11) {
+    dguide.alloc((kCdfGuide + 1) * sizeof(int));
+    buildCdfGuideDevice((const float*)daux.ptr, auxN, 0, 1, (int*)dguide.ptr, 0);
+  }
   stKernel<<<(n + 127) / 128, 128>>>(which, din.ptr, n, dout.ptr, (const float*)daux.ptr, auxN, auxW,
-                                     auxH);
+                                     auxH, (const int*)dguide.ptr);
   cudaCheck(cudaGetLastError(), "selftest launch");
   cudaCheck(cudaDeviceSynchronize(), "selftest");
   cudaCheck(cudaMemcpy(out, dout.ptr, ob * n, cudaMemcpyDeviceToHost), "selftest download");

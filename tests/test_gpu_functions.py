@@ -99,6 +99,47 @@ def test_cdf_search_bit_exact(lib):
     assert np.array_equal(got["index"], ref["index"])
 
 
+def search_on_device(lib, which, u, cdf):
+    """Indices of u in cdf by self-test function `which` (9 plain, 11 guided)."""
+    u = np.asarray(u, np.float32)
+    cdf = np.asarray(cdf, np.float32)
+    payload = u.tobytes() + np.int32(len(cdf)).tobytes() + cdf.tobytes()
+    out = np.zeros(len(u), np.int32)
+    rc = lib.sundog_selftest(which, ctypes.create_string_buffer(payload, len(payload)), len(u),
+                             out.ctypes.data, out.nbytes)
+    assert rc == 0, lib.sundog_last_error()
+    return out
+
+
+def test_cdf_search_guided_matches_plain(lib):
+    """The guided search (the environment's tables) returns the plain search's
+    index: on the golden vectors bit for bit, and on CDFs with long flat runs
+    (zero-luminance texels) at every guide bucket boundary and its float
+    neighbours, where a wrong bracket would show."""
+    which, n, payload, ref = golden("cdf_search")
+    got = device(lib, 11, payload, n, ref.dtype)
+    assert np.array_equal(got["index"], ref["index"])
+    rng = np.random.default_rng(7)
+    K = 256
+    bounds = np.arange(K + 1, dtype=np.float32) / K
+    u = np.concatenate([bounds[:-1], np.nextafter(bounds[1:], 0.0), np.nextafter(bounds[:-1], 1.0),
+                        rng.random(20000).astype(np.float32)])
+    u = u[(u >= 0.0) & (u < 1.0)]
+    for trial in range(4):
+        n_entries = [3, 65, 513, 1025][trial]
+        w = rng.random(n_entries - 1)
+        w[rng.random(n_entries - 1) < 0.6] = 0.0  # flat runs
+        w[0] = 0.0
+        w[-1] = max(w[-1], 0.1)
+        c = np.concatenate([[0.0], np.cumsum(w) / np.sum(w)]).astype(np.float32)
+        c[-1] = 1.0
+        u_all = np.concatenate([u, c[:-1], np.nextafter(c[:-1], 0.0).astype(np.float32)])
+        u_all = u_all[(u_all >= 0.0) & (u_all < 1.0)]
+        plain = search_on_device(lib, 9, u_all, c)
+        guided = search_on_device(lib, 11, u_all, c)
+        assert np.array_equal(plain, guided), "cdf of %d entries" % n_entries
+
+
 def test_bsdf_eval_pdf(lib):
     which, n, payload, ref = golden("bsdf_eval")
     got = device(lib, which, payload, n, ref.dtype)
