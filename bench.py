@@ -560,14 +560,19 @@ def run_ours(args):
                                                ctypes.byref(rr)), "render_ex", lib)  # warm
                 h0, d0 = ctypes.c_uint64(), ctypes.c_uint64()
                 lib.sundog_transfer_bytes(ctypes.byref(h0), ctypes.byref(d0))
-                e_steps = max(1, min(args.steps, 3))
+                # Up to 5 calls: a single slow driver call (tens to hundreds of
+                # ms, at random on this hardware) then moves the mean less.
+                e_steps = max(1, min(args.steps, 5))
                 if dist:
                     dist.barrier()
                 t0 = time.perf_counter()
                 erays = 0
+                calls = []
                 for _ in range(e_steps):
+                    tc = time.perf_counter()
                     abi.check(lib.sundog_render_ex(h, ctypes.byref(o), ctypes.byref(ext),
                                                    ctypes.byref(rr)), "render_ex", lib)
+                    calls.append(1000.0 * (time.perf_counter() - tc))
                     erays += rr.rays_traced
                 et = time.perf_counter() - t0
                 h1, d1 = ctypes.c_uint64(), ctypes.c_uint64()
@@ -582,7 +587,9 @@ def run_ours(args):
                     "d2h_bytes_per_step": int(db / e_steps),
                     "ms_per_step": 1000.0 * et / e_steps,
                     "last_call_ms": {"load": rr.load_ms, "build": rr.build_ms,
-                                     "render": rr.render_ms, "total": rr.total_ms}}
+                                     "render": rr.render_ms, "total": rr.total_ms},
+                    "call_ms": {"min": min(calls), "median": float(np.median(calls)),
+                                "max": max(calls)}}
         plain = e2e_run(False)
         e2e = e2e_run(True)
         e2e["path"] = ("sundog_set_device_memory_cache(1) once, then sundog_render_ex per step "
@@ -591,7 +598,7 @@ def run_ours(args):
                        "slowest rank")
         e2e["default_memory_settings"] = {
             "value": plain["value"], "ms_per_step": plain["ms_per_step"],
-            "last_call_ms": plain["last_call_ms"],
+            "last_call_ms": plain["last_call_ms"], "call_ms": plain["call_ms"],
             "note": "the library's default: every device buffer allocated and freed inside "
                     "each call, as the reference's render does"}
 
