@@ -113,8 +113,11 @@ __device__ __forceinline__ bool serveStartW(unsigned long long id, Path& p, int&
 // slot empty when the frame's paths are used up. Record passes (GUIDE &
 // kGuideRecord) start the slot's trail empty.
 template <int GUIDE>
-__device__ __forceinline__ void refill(int slot, int out) {
+__device__ __forceinline__ void refill(int slot, int out, bool start = false) {
   const WfPool& pool = c_pool;
+  // When the start stage placed every path, a slot whose path ends has no id
+  // left to take: skip the atomic on the path counter that would say so.
+  if (!start && !pool.refillOpen) return;
   const unsigned long long numPaths = (GUIDE & kWfServe) ? c_wbatch.numPaths : c_wlp.numPaths;
   while (true) {
     unsigned long long id = nextPathId<GUIDE>();
@@ -153,7 +156,7 @@ __global__ void __launch_bounds__(kRenderBlock) wfStart() {
   const WfPool& pool = c_pool;
   for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < pool.cap;
        slot += gridDim.x * blockDim.x)
-    refill<GUIDE>(slot, 0);
+    refill<GUIDE>(slot, 0, true);
 }
 
 // Camera paths into the pool without atomics, for frames whose 8x8 pixel
@@ -762,6 +765,7 @@ static int runPool(WfBuffers& b, cudaStream_t st, unsigned long long numPaths, i
   pool.trails = (PoolSlot<GuideTrail>*)b.trails.ptr;
   pool.jobs = (unsigned char*)b.jobs;
   pool.cap = (int)std::min<unsigned long long>((unsigned long long)b.cap, numPaths);
+  pool.refillOpen = (unsigned long long)pool.cap < numPaths ? 1 : 0;
   cudaCheck(cudaMemcpyToSymbolAsync(c_pool, &pool, sizeof pool, 0, cudaMemcpyHostToDevice, st),
             "wavefront pool");
   cudaCheck(cudaMemsetAsync(b.counts.ptr, 0, b.counts.bytes, st), "wavefront counts");

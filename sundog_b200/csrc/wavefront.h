@@ -39,6 +39,7 @@ struct WfPool {
   PoolSlot<GuideTrail>* trails;  // guided vertices awaiting their path's end (record passes)
   unsigned char* jobs;     // serving batches: the job slot of each slot's path
   int cap;
+  int refillOpen;          // 0: every path of the launch fits the pool at once (no refills)
 };
 
 // Host-owned pool storage, grown on demand.
