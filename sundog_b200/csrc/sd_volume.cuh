@@ -43,18 +43,18 @@ SDB_HD float latticeValue(int x, int y, int z, unsigned seed) {
   return (float)h * (1.0f / 4294967296.0f);
 }
 
-// Trilinear value noise with smoothstep fade. (device/noise.cuh:32-50)
-SDB_HD float valueNoise(float3 p, unsigned seed) {
-  float fx = floorf(p.x), fy = floorf(p.y), fz = floorf(p.z);
-  int ix = (int)fx, iy = (int)fy, iz = (int)fz;
-  float tx = p.x - fx, ty = p.y - fy, tz = p.z - fz;
-  tx = tx * tx * (3.0f - 2.0f * tx);
-  ty = ty * ty * (3.0f - 2.0f * ty);
-  tz = tz * tz * (3.0f - 2.0f * tz);
-  float c000 = latticeValue(ix, iy, iz, seed), c100 = latticeValue(ix + 1, iy, iz, seed);
-  float c010 = latticeValue(ix, iy + 1, iz, seed), c110 = latticeValue(ix + 1, iy + 1, iz, seed);
-  float c001 = latticeValue(ix, iy, iz + 1, seed), c101 = latticeValue(ix + 1, iy, iz + 1, seed);
-  float c011 = latticeValue(ix, iy + 1, iz + 1, seed), c111 = latticeValue(ix + 1, iy + 1, iz + 1, seed);
+// Smoothstep fade of the fractional part; f receives the cell's floor.
+SDB_HD float fadeFrac(float x, int& f) {
+  float fx = floorf(x);
+  f = (int)fx;
+  float t = x - fx;
+  return t * t * (3.0f - 2.0f * t);
+}
+
+// Trilinear blend of a cell's eight lattice values (cYZX naming: c100 is
+// x + 1), x first, then y, then z.
+SDB_HD float trilerp(float c000, float c100, float c010, float c110, float c001, float c101,
+                     float c011, float c111, float tx, float ty, float tz) {
   float x00 = c000 + (c100 - c000) * tx;
   float x10 = c010 + (c110 - c010) * tx;
   float x01 = c001 + (c101 - c001) * tx;
@@ -62,6 +62,25 @@ SDB_HD float valueNoise(float3 p, unsigned seed) {
   float y0 = x00 + (x10 - x00) * ty;
   float y1 = x01 + (x11 - x01) * ty;
   return y0 + (y1 - y0) * tz;
+}
+
+// The same blend on the plane y == 0 (y fade 0: each y lerp returns its
+// lower end, a + (b - a) * 0 == a for the finite lattice values).
+SDB_HD float bilerpXZ(float c000, float c100, float c001, float c101, float tx, float tz) {
+  float x00 = c000 + (c100 - c000) * tx;
+  float x01 = c001 + (c101 - c001) * tx;
+  return x00 + (x01 - x00) * tz;
+}
+
+// Trilinear value noise with smoothstep fade. (device/noise.cuh:32-50)
+SDB_HD float valueNoise(float3 p, unsigned seed) {
+  int ix, iy, iz;
+  float tx = fadeFrac(p.x, ix), ty = fadeFrac(p.y, iy), tz = fadeFrac(p.z, iz);
+  return trilerp(latticeValue(ix, iy, iz, seed), latticeValue(ix + 1, iy, iz, seed),
+                 latticeValue(ix, iy + 1, iz, seed), latticeValue(ix + 1, iy + 1, iz, seed),
+                 latticeValue(ix, iy, iz + 1, seed), latticeValue(ix + 1, iy, iz + 1, seed),
+                 latticeValue(ix, iy + 1, iz + 1, seed), latticeValue(ix + 1, iy + 1, iz + 1, seed),
+                 tx, ty, tz);
 }
 
 // Three octaves, lacunarity 2.03, gain 0.5. (device/noise.cuh:53-61)
@@ -80,16 +99,10 @@ SDB_HD float fbm3(float3 p, unsigned seed) {
 // finite lattice values) and the four lattice values at iy + 1 never count.
 // The same value from half the hashes.
 SDB_HD float valueNoiseY0(float3 p, unsigned seed) {
-  float fx = floorf(p.x), fz = floorf(p.z);
-  int ix = (int)fx, iz = (int)fz;
-  float tx = p.x - fx, tz = p.z - fz;
-  tx = tx * tx * (3.0f - 2.0f * tx);
-  tz = tz * tz * (3.0f - 2.0f * tz);
-  float c000 = latticeValue(ix, 0, iz, seed), c100 = latticeValue(ix + 1, 0, iz, seed);
-  float c001 = latticeValue(ix, 0, iz + 1, seed), c101 = latticeValue(ix + 1, 0, iz + 1, seed);
-  float x00 = c000 + (c100 - c000) * tx;
-  float x01 = c001 + (c101 - c001) * tx;
-  return x00 + (x01 - x00) * tz;
+  int ix, iz;
+  float tx = fadeFrac(p.x, ix), tz = fadeFrac(p.z, iz);
+  return bilerpXZ(latticeValue(ix, 0, iz, seed), latticeValue(ix + 1, 0, iz, seed),
+                  latticeValue(ix, 0, iz + 1, seed), latticeValue(ix + 1, 0, iz + 1, seed), tx, tz);
 }
 
 // fbm3 of a point on the plane y == 0 (the wave height field): the first
@@ -103,6 +116,102 @@ SDB_HD float fbm3Y0(float3 p, unsigned seed) {
   return sum;
 }
 
+// The four heights of waveNormal's central differences, fbm3Y0 at
+// (x +- e, 0, z) and (x, 0, z +- e), with the lattice values they share read
+// once. Per octave the four points' coordinates come from the same
+// arithmetic as fbm3Y0's, so the x samples share z and the z samples share
+// x, and all share y; e is under half a lattice cell at every octave (0.05,
+// 0.10, 0.21), so the x pair spans the cells ixm and ixm + 1 along x and the
+// z pair izm and izm + 1 along z (the centre's cells lie between). Block A
+// holds x = ixm .. ixm + 2 at the x samples' z cells (izc, izc + 1); the z
+// samples' x cells (ixc = ixm or ixm + 1) are inside it, and of their z
+// values izm .. izm + 2 block A has the two at izc, izc + 1, so one more
+// z row (E) completes them: 16 lattice values instead of 32 per octave (8
+// instead of 16 on the plane y == 0). Each sample then blends its own
+// cell's eight values with its own fade weights, exactly as valueNoise.
+SDB_HD void waveHeights(float3 p, float e, unsigned seed, float& hx1, float& hx0, float& hz1,
+                        float& hz0) {
+  float3 qxp = p + v3(e, 0.0f, 0.0f), qxm = p - v3(e, 0.0f, 0.0f);
+  float3 qzp = p + v3(0.0f, 0.0f, e), qzm = p - v3(0.0f, 0.0f, e);
+  float sxp = 0.0f, sxm = 0.0f, szp = 0.0f, szm = 0.0f;
+  for (int oct = 0; oct < 3; oct++) {
+    const unsigned sd = seed + (unsigned)oct * 101u;
+    int ixp, ixm, ixc, izc, izp, izm, iy = 0;
+    const float txp = fadeFrac(qxp.x, ixp), txm = fadeFrac(qxm.x, ixm), txc = fadeFrac(qzp.x, ixc);
+    const float tzc = fadeFrac(qxp.z, izc), tzp = fadeFrac(qzp.z, izp), tzm = fadeFrac(qzm.z, izm);
+    const float ty = oct == 0 ? 0.0f : fadeFrac(qxp.y, iy);
+    const int ny = oct == 0 ? 1 : 2;  // y rows that count (one on y == 0)
+    // A[dx][dy][dz]: x = ixm + dx, y = iy + dy, z = izc + dz.
+    float A[3][2][2];
+#pragma unroll
+    for (int dx = 0; dx < 3; dx++)
+#pragma unroll
+      for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+        for (int dz = 0; dz < 2; dz++)
+          A[dx][dy][dz] = dy < ny ? latticeValue(ixm + dx, iy + dy, izc + dz, sd) : 0.0f;
+    // E[dx][dy]: the z samples' remaining z row, x = ixc + dx.
+    const int zE = izc == izm ? izm + 2 : izm;
+    float E[2][2];
+#pragma unroll
+    for (int dx = 0; dx < 2; dx++)
+#pragma unroll
+      for (int dy = 0; dy < 2; dy++)
+        E[dx][dy] = dy < ny ? latticeValue(ixc + dx, iy + dy, zE, sd) : 0.0f;
+    // The z samples' column at x = ixc + dx: z = izc, izc + 1 from A, zE from E.
+    const bool oc = ixc != ixm;
+    auto col = [&](int dx, int dy, int z) -> float {
+      const float a0 = oc ? A[dx + 1][dy][0] : A[dx][dy][0];
+      const float a1 = oc ? A[dx + 1][dy][1] : A[dx][dy][1];
+      return z == izc ? a0 : (z == izc + 1 ? a1 : E[dx][dy]);
+    };
+    const bool ob = ixp != ixm;
+    float v[4];
+    if (oct == 0) {
+      v[0] = bilerpXZ(ob ? A[1][0][0] : A[0][0][0], ob ? A[2][0][0] : A[1][0][0],
+                      ob ? A[1][0][1] : A[0][0][1], ob ? A[2][0][1] : A[1][0][1], txp, tzc);
+      v[1] = bilerpXZ(A[0][0][0], A[1][0][0], A[0][0][1], A[1][0][1], txm, tzc);
+      v[2] = bilerpXZ(col(0, 0, izp), col(1, 0, izp), col(0, 0, izp + 1), col(1, 0, izp + 1), txc,
+                      tzp);
+      v[3] = bilerpXZ(col(0, 0, izm), col(1, 0, izm), col(0, 0, izm + 1), col(1, 0, izm + 1), txc,
+                      tzm);
+    } else {
+      v[0] = trilerp(ob ? A[1][0][0] : A[0][0][0], ob ? A[2][0][0] : A[1][0][0],
+                     ob ? A[1][1][0] : A[0][1][0], ob ? A[2][1][0] : A[1][1][0],
+                     ob ? A[1][0][1] : A[0][0][1], ob ? A[2][0][1] : A[1][0][1],
+                     ob ? A[1][1][1] : A[0][1][1], ob ? A[2][1][1] : A[1][1][1], txp, ty, tzc);
+      v[1] = trilerp(A[0][0][0], A[1][0][0], A[0][1][0], A[1][1][0], A[0][0][1], A[1][0][1],
+                     A[0][1][1], A[1][1][1], txm, ty, tzc);
+      v[2] = trilerp(col(0, 0, izp), col(1, 0, izp), col(0, 1, izp), col(1, 1, izp),
+                     col(0, 0, izp + 1), col(1, 0, izp + 1), col(0, 1, izp + 1),
+                     col(1, 1, izp + 1), txc, ty, tzp);
+      v[3] = trilerp(col(0, 0, izm), col(1, 0, izm), col(0, 1, izm), col(1, 1, izm),
+                     col(0, 0, izm + 1), col(1, 0, izm + 1), col(0, 1, izm + 1),
+                     col(1, 1, izm + 1), txc, ty, tzm);
+    }
+    const float amp = oct == 0 ? 0.5f : (oct == 1 ? 0.25f : 0.125f);
+    if (oct == 0) {
+      sxp = amp * v[0];
+      sxm = amp * v[1];
+      szp = amp * v[2];
+      szm = amp * v[3];
+    } else {
+      sxp += amp * v[0];
+      sxm += amp * v[1];
+      szp += amp * v[2];
+      szm += amp * v[3];
+    }
+    qxp = 2.03f * qxp + v3(11.7f, 5.3f, 7.9f);
+    qxm = 2.03f * qxm + v3(11.7f, 5.3f, 7.9f);
+    qzp = 2.03f * qzp + v3(11.7f, 5.3f, 7.9f);
+    qzm = 2.03f * qzm + v3(11.7f, 5.3f, 7.9f);
+  }
+  hx1 = sxp;
+  hx0 = sxm;
+  hz1 = szp;
+  hz0 = szm;
+}
+
 // Wave normal from an fBm height field over world xz by central differences;
 // falls back to ns when the perturbed normal would face away from wo.
 // (device/noise.cuh:67-79)
@@ -110,8 +219,18 @@ SDB_COLD float3 waveNormal(float3 x, float3 ns, float3 wo, float amp, float freq
   const unsigned seed = 1337u;
   const float e = 0.05f;
   float3 p = v3(x.x * freq, 0.0f, x.z * freq);
-  float hx1 = fbm3Y0(p + v3(e, 0.0f, 0.0f), seed), hx0 = fbm3Y0(p - v3(e, 0.0f, 0.0f), seed);
-  float hz1 = fbm3Y0(p + v3(0.0f, 0.0f, e), seed), hz0 = fbm3Y0(p - v3(0.0f, 0.0f, e), seed);
+  float hx1, hx0, hz1, hz0;
+  // Below 2^20 every octave's coordinates keep a float spacing of at most
+  // 0.5, so each pair of samples spans at most two cells, as waveHeights
+  // needs; farther out the four fBm sums are taken one by one.
+  if (fabsf(p.x) < 1048576.0f && fabsf(p.z) < 1048576.0f) {
+    waveHeights(p, e, seed, hx1, hx0, hz1, hz0);
+  } else {
+    hx1 = fbm3Y0(p + v3(e, 0.0f, 0.0f), seed);
+    hx0 = fbm3Y0(p - v3(e, 0.0f, 0.0f), seed);
+    hz1 = fbm3Y0(p + v3(0.0f, 0.0f, e), seed);
+    hz0 = fbm3Y0(p - v3(0.0f, 0.0f, e), seed);
+  }
   float dhdx = (hx1 - hx0) / (2.0f * e);
   float dhdz = (hz1 - hz0) / (2.0f * e);
   float side = ns.y >= 0.0f ? 1.0f : -1.0f;
