@@ -210,12 +210,14 @@ __device__ __forceinline__ void putHit(PoolSlot<TraceHit>& s, float t, int inst,
 #ifndef SDB_WF_INNER_MIN
 #define SDB_WF_INNER_MIN 4
 #endif
-// Idle lanes a warp gathers before it fetches new rays (measured on the
-// instancing frame: 894 Mrays/s at 24, 869 with a grid-stride loop, 752 when
-// every idle lane fetches at once: fresh rays at the TLAS root diverge from
-// the warp's deep BLAS walks).
+// Idle lanes a warp gathers before it fetches new rays (on the instancing
+// frame with the one-action loop: 894 Mrays/s at 24, 869 with a grid-stride
+// loop, 752 when every idle lane fetches at once: fresh rays at the TLAS
+// root diverge from the warp's deep BLAS walks; with the 4-wide walk and
+// descent runs, config 1 / config 0: 1,717 / 2,798 at 20, 1,706 / 2,801 at
+// 24, 1,678 / 2,799 at 28).
 #ifndef SDB_WF_FETCH_IDLE
-#define SDB_WF_FETCH_IDLE 24
+#define SDB_WF_FETCH_IDLE 20
 #endif
 
 // Radiance rays with dynamic ray fetch (Aila and Laine, "Understanding the
