@@ -68,6 +68,12 @@ __device__ __forceinline__ const SdLaunch& slotLaunch(int slot) {
 #ifndef SDB_WF_SHADE_BLOCKS
 #define SDB_WF_SHADE_BLOCKS 5
 #endif
+// The second shading stage alone at 6 blocks (80 registers): config 1
+// 1,718 -> 1,729 Mrays/s, config 0 2,756 -> 2,779, config 2 and the gallery
+// scenes within 0.2%.
+#ifndef SDB_WF_SHADEB_BLOCKS
+#define SDB_WF_SHADEB_BLOCKS 6
+#endif
 
 // Slot index for an append to a list by the calling lanes together.
 __device__ __forceinline__ unsigned appendSlot(unsigned* count) {
@@ -598,7 +604,7 @@ __global__ void wfShadowFetch() {}
 // (sd_guide.cuh; the mixture table is in the launch block). GUIDE &
 // kGuideRecord: the guided vertex joins the slot's trail.
 template <int GUIDE>
-__global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADE_BLOCKS) wfShadeB(int in, int out) {
+__global__ void __launch_bounds__(kRenderBlock, SDB_WF_SHADEB_BLOCKS) wfShadeB(int in, int out) {
   const WfPool& pool = c_pool;
   const unsigned n = pool.counts[in];
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
